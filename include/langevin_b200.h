@@ -1,0 +1,215 @@
+/*
+ * langevin_b200.h — C-ABI of the B200 (sm_100a) heavy-quark Langevin engine.
+ *
+ * Drop-in boundary for the per-particle Langevin time loop of LangevInMedium.jl.
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (0 = LIM_OK, negative = error class) and never throws across the ABI.  The
+ * text of the last error is returned by lim_last_error().
+ *
+ * Host-side array layout is the reference's Julia layout: a (rows, N) matrix in
+ * column-major order, i.e. one particle's components are contiguous:
+ *     x[d + rows * i]   for component d of particle i.
+ * Medium tables (Nr, Nt) are column-major too: T[i + Nr * j] is T(xgrid[i], tgrid[j]).
+ * Host memory is always owned by the caller; device memory is owned by the
+ * context until lim_destroy().
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   - src/simulate.jl:21-87 and src/simulate_gpu_wrapper.jl:15-72
+ *       simulate_ensemble_bulk(::CPUBackend / ::GPUBackend, r_grid, p_grid,
+ *       dens, Tfield, Vfield, (xgrid, tgrid); kwargs...)
+ *   - src/simulate.jl:117-141 (CPU_GCBackend, Milne (tau, r) coordinates)
+ *   - src/simulate_cpu.jl:215-316 / src/simulate_gpu.jl:283-392 (the step loop)
+ *   - src/simulate_cpu_general_coords.jl:83-126 (the Milne step loop)
+ * A Julia caller reaches these through ccall.
+ */
+#ifndef LANGEVIN_B200_H
+#define LANGEVIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LIM_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------- */
+enum {
+    LIM_OK              = 0,
+    LIM_ERR_ARG         = -1,  /* invalid argument (the reference's error(...) on bad input) */
+    LIM_ERR_CUDA        = -2,  /* a CUDA runtime call failed */
+    LIM_ERR_STATE       = -3,  /* call out of order (e.g. run before upload) */
+    LIM_ERR_NONFINITE   = -4,  /* NaN/Inf in the particle state (simulate_cpu.jl:293-303) */
+    LIM_ERR_TIMEOUT     = -5,  /* a bounded device-side wait gave up */
+    LIM_ERR_UNSUPPORTED = -6,  /* option combination the engine does not provide */
+    LIM_ERR_NOMEM       = -7   /* device or host allocation failed */
+};
+
+/* ---- enumerations used in lim_params -------------------------------------- */
+enum { LIM_FP64 = 0, LIM_FP32 = 1 };                    /* precision of the particle arithmetic */
+enum { LIM_COORDS_CARTESIAN = 0, LIM_COORDS_MILNE = 1 }; /* kernels_cpu.jl vs kernels_cpu_GC.jl */
+enum {
+    LIM_COLL_LANGEVIN     = 0,  /* exact-OU drag + kick (simulate_cpu.jl:252-277) */
+    LIM_COLL_RTA          = 1,  /* BGK/RTA resampling (simulate_cpu.jl:234-251, GPU form kernels_gpu.jl:653-704) */
+    LIM_COLL_LANGEVIN_RTA = 2,  /* OU kick then RTA resample in the same LRF step (new; not a reference mode) */
+    LIM_COLL_FLUID        = 3   /* momentum_langevin=false or DsT==0: set_to_fluid_velocity (simulate_cpu.jl:229-233) */
+};
+enum {
+    LIM_MEDIUM_RT      = 0,     /* reference (r, t) tables, bilinear (kernels_cpu.jl:22-51) */
+    LIM_MEDIUM_BJORKEN = 1,     /* analytic T(tau) = T0 (tau0/tau)^p, zero transverse flow */
+    LIM_MEDIUM_GRID    = 2      /* 2+1D grid T, u^x, u^y on (tau, x, y), trilinear */
+};
+enum { LIM_SPLINE_DRAG = 0, LIM_SPLINE_RTA = 1 };       /* transport.jl:208-222 */
+enum {                                                   /* observables reduced in FP64 on device */
+    LIM_OBS_COUNT = 0,        /* number of particles counted (alive, or frozen-out when fo mode) */
+    LIM_OBS_MEAN_PT,          /* <sqrt(px^2+py^2)> */
+    LIM_OBS_MEAN_COS2PHI,     /* <cos 2 phi_p> = <(px^2-py^2)/pT^2> */
+    LIM_OBS_FRAC_PT_GT,       /* fraction with pT > obs_pt_cut (sharp) */
+    LIM_OBS_FRAC_PT_GT_SMOOTH,/* <sigmoid((pT - cut)/width)> */
+    LIM_OBS_MEAN_P2,          /* <|p|^2> over all momentum rows */
+    LIM_OBS_MEAN_E,           /* <sqrt(m^2+|p|^2)> */
+    LIM_OBS_MEAN_LAM1_NUM,    /* <(m/E) |p|^2> (lambda_1 numerator, test_momentum_dims3.jl:74-78) */
+    LIM_OBS_MEAN_PX,          /* <p_x> */
+    LIM_OBS_MEAN_WPX,         /* <(m/E) p_x> */
+    LIM_OBS_MEAN_PZ2,         /* <p_z^2> (row 3) */
+    LIM_OBS_MEAN_X2,          /* <sum_d x_d^2> over position rows */
+    LIM_OBS_NUM               /* number of observables written by lim_observables */
+};
+
+/*
+ * Run configuration.  Every field is 8 bytes wide so that the struct has the
+ * same layout in C, Julia (an isbits struct of Float64/Int64) and Python ctypes.
+ * Field meanings follow the reference keyword arguments
+ * (simulate_gpu_wrapper.jl:23-52).
+ */
+typedef struct lim_params {
+    double  dt;                 /* Δt [fm/c] */
+    double  t0;                 /* initial_time; medium time at step s is s*dt + t0 */
+    double  m;                  /* heavy-quark mass [GeV] */
+    double  DsT;                /* DsT; <= 0 disables the drag (kernels_cpu.jl:270) */
+    double  Tfo;                /* freeze-out temperature for the latch (kernels_gpu.jl:588-635) */
+    double  psi2;               /* event-plane angle of the optional v2 modulation */
+    double  obs_pt_cut;         /* pT threshold of LIM_OBS_FRAC_PT_GT[_SMOOTH] [GeV] */
+    double  obs_pt_width;       /* sigmoid width of LIM_OBS_FRAC_PT_GT_SMOOTH [GeV] */
+    int64_t dims;               /* position rows: 1 (radial mode), 2 or 3; Milne: 2 = (tau, r) */
+    int64_t pdim;               /* momentum rows (momentum_dimensions resolved; 0 => dims) */
+    int64_t coords;             /* LIM_COORDS_* */
+    int64_t collision;          /* LIM_COLL_* */
+    int64_t relativistic;       /* 1: Lorentz boosts, drag eta*m/E, stream p/E; 0: Galilean, eta, p/m */
+    int64_t bjorken_redshift;   /* 1: p_z *= tau_a/(tau_a+dt) in the LRF (kernels_cpu.jl:427-435) */
+    int64_t position_diffusion; /* 1: x += sqrt(2 D dt) xi with D = DsT/T/fmGeV (kernels_cpu.jl:592-607) */
+    int64_t reflecting_boundary;/* 1: reflect at r_max = last(xgrid) (kernels_cpu.jl:609-634) */
+    int64_t integrator_mode;    /* 0: pre-point exact OU; 1: drift-midpoint (kernels_gpu.jl:368-381) */
+    int64_t freezeout_capture;  /* 1: latch state at the first T < Tfo */
+    int64_t freezeout_interp;   /* 1: interpolate the latch linearly in T to T = Tfo */
+    int64_t precision;          /* LIM_FP64 or LIM_FP32 */
+    int64_t seed;               /* Philox-4x32-10 key (64 bit) */
+    int64_t particle_offset;    /* global id of particle 0 (shards keep the global noise stream) */
+    int64_t stop_after_freezeout; /* 1: stop evolving a particle once latched (fo outputs unchanged) */
+    int64_t block_size;         /* threads per block of the step kernel; 0 = autotuned default */
+} lim_params;
+
+typedef struct lim_ctx lim_ctx;
+
+/* ---- context ---------------------------------------------------------------- */
+int         lim_abi_version(void);
+/* Create a context on CUDA device `device`.  `stream` is a cudaStream_t (may be
+ * NULL for a private stream), so the engine can share a caller's stream
+ * (CUDA.jl: CUDA.stream().handle). */
+int         lim_create(int device, void* stream, lim_ctx** out);
+int         lim_destroy(lim_ctx* ctx);
+/* Text of the last error on this context (or of the last failed lim_create when
+ * ctx is NULL).  Valid until the next call on the same context. */
+const char* lim_last_error(const lim_ctx* ctx);
+int         lim_synchronize(lim_ctx* ctx);
+/* Bytes of device memory the context currently holds. */
+int         lim_device_bytes(const lim_ctx* ctx, int64_t* bytes);
+
+/* ---- configuration ------------------------------------------------------------ */
+int lim_set_params(lim_ctx* ctx, const lim_params* params);
+
+/* Reference (r, t) medium: xgrid (nr, ascending), tgrid (nt, ascending),
+ * T and V column-major (nr, nt); V2 (nr, nt) or NULL (no v2 modulation).
+ * Replaces the CuArray uploads of simulate_gpu.jl:81-88. */
+int lim_set_medium_rt(lim_ctx* ctx,
+                      const double* xgrid, int64_t nr,
+                      const double* tgrid, int64_t nt,
+                      const double* T, const double* V, const double* V2);
+
+/* Analytic Bjorken medium: T(tau) = T0 * (tau0 / tau)^power for tau >= tau0
+ * (T0 for tau < tau0), zero transverse flow.  r_max bounds reflection. */
+int lim_set_medium_bjorken(lim_ctx* ctx, double T0, double tau0, double power, double r_max);
+
+/* 2+1D medium on a uniform grid: fields in FP32, row-major [it][iy][ix]
+ * (ix fastest), node (ix, iy, it) at (x0 + ix*dx, y0 + iy*dy, tau0 + it*dtau).
+ * u^x, u^y are flow velocities (not four-velocity components). */
+int lim_set_medium_grid(lim_ctx* ctx,
+                        int64_t nx, int64_t ny, int64_t nt,
+                        double x0, double dx, double y0, double dy,
+                        double tau0, double dtau,
+                        const float* T, const float* ux, const float* uy);
+
+/* Uniform-grid linear spline of a transport time in fm (transport.jl:165-253):
+ * vals[k] at T = Tmin + k/invdT, k = 0..n-1.  which = LIM_SPLINE_DRAG (the drag
+ * time 1/eta_D) or LIM_SPLINE_RTA (the RTA relaxation time). */
+int lim_set_spline(lim_ctx* ctx, int which, double Tmin, double invdT,
+                   const double* vals, int64_t n);
+
+/* Jüttner inverse-CDF table (transport.jl:277-365): vals[jT*nU + iu] = p*(u_iu; T_jT). */
+int lim_set_invcdf(lim_ctx* ctx, const double* vals, int64_t nU, int64_t nT,
+                   double Tmin, double invdT);
+
+/* ---- particle state ----------------------------------------------------------- */
+/* x: (dims, n) and p: (pdim, n) column-major host arrays (the Julia layout).
+ * Resets the freeze-out latch and the non-finite status. */
+int lim_upload_state(lim_ctx* ctx, const double* x, int64_t dims,
+                     const double* p, int64_t pdim, int64_t n);
+int lim_download_state(lim_ctx* ctx, double* x, double* p);
+
+/* The step-0 lab boost applied before the loop (simulate_cpu.jl:160-163). */
+int lim_initial_lab_boost(lim_ctx* ctx);
+
+/* Advance steps first_step .. first_step+nsteps-1 (medium time s*dt + t0).
+ * When save_every > 0 and hist_x / hist_p are not NULL, the state after every
+ * step s with s % save_every == 0 is written to snapshot slot
+ * (s / save_every) - first_slot of the host arrays hist_x (dims, n, nslots)
+ * and hist_p (pdim, n, nslots), column-major.  Returns LIM_ERR_NONFINITE (and
+ * the first bad step in lim_status) if any particle became NaN/Inf. */
+int lim_run(lim_ctx* ctx, int64_t first_step, int64_t nsteps,
+            int64_t save_every, int64_t first_slot,
+            double* hist_x, double* hist_p);
+
+/* First step at which a particle became non-finite, or -1. */
+int lim_status(lim_ctx* ctx, int64_t* first_bad_step);
+
+/* Freeze-out latch outputs (simulate_gpu.jl:395-396): fo_pos (dims, n),
+ * fo_mom (pdim, n), fo_tau (n), fo_flag (n, 1.0 = latched). */
+int lim_download_freezeout(lim_ctx* ctx, double* fo_pos, double* fo_mom,
+                           double* fo_tau, double* fo_flag);
+
+/* FP64 device reduction of the current state (or of the freeze-out latch when
+ * from_freezeout != 0): out[LIM_OBS_NUM] (see the LIM_OBS_* enumeration). */
+int lim_observables(lim_ctx* ctx, int from_freezeout, double* out);
+
+/* Debug/parity mode: record every random variate the kernel consumes into a
+ * device buffer of nsteps * LIM_NOISE_SLOTS * n doubles, laid out
+ * [step - first_step][slot][particle]; lim_download_noise copies it out.
+ * Pass nsteps = 0 to switch recording off. */
+#define LIM_NOISE_SLOTS 11
+int lim_record_noise(lim_ctx* ctx, int64_t first_step, int64_t nsteps);
+int lim_download_noise(lim_ctx* ctx, double* out);
+
+/* Philox-4x32-10 block as the device computes it (for host-side parity checks):
+ * out[4] = philox(ctr[4], key[2]). */
+int lim_philox_device(lim_ctx* ctx, const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* ---- timing helpers (bench) ---------------------------------------------------- */
+/* Device time of the last lim_run's step kernels in ms (CUDA events on the
+ * context stream) and the number of kernel launches it issued. */
+int lim_last_run_stats(lim_ctx* ctx, double* kernel_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LANGEVIN_B200_H */

@@ -1,0 +1,302 @@
+"""ctypes binding of ``liblangevin_b200.so`` (the C-ABI declared in include/langevin_b200.h).
+
+This is the Python twin of the Julia ``ccall`` layer: plain pointers and sizes, an
+``int`` status per call, and ``lim_last_error`` turned into an exception.  There is
+no fallback: if the CUDA library is missing or no GPU is present, the calls fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "liblangevin_b200.so"
+HEADER = PKG_DIR.parent / "include" / "langevin_b200.h"
+
+LIM_OK, LIM_ERR_ARG, LIM_ERR_CUDA, LIM_ERR_STATE, LIM_ERR_NONFINITE, LIM_ERR_TIMEOUT, LIM_ERR_UNSUPPORTED, LIM_ERR_NOMEM = \
+    0, -1, -2, -3, -4, -5, -6, -7
+LIM_FP64, LIM_FP32 = 0, 1
+LIM_COORDS_CARTESIAN, LIM_COORDS_MILNE = 0, 1
+LIM_COLL_LANGEVIN, LIM_COLL_RTA, LIM_COLL_LANGEVIN_RTA, LIM_COLL_FLUID = 0, 1, 2, 3
+LIM_SPLINE_DRAG, LIM_SPLINE_RTA = 0, 1
+LIM_NOISE_SLOTS = 11
+OBS_NAMES = ("count", "mean_pt", "mean_cos2phi", "frac_pt_gt", "frac_pt_gt_smooth", "mean_p2", "mean_E",
+             "mean_lam1_num", "mean_px", "mean_wpx", "mean_pz2", "mean_x2")
+LIM_OBS_NUM = len(OBS_NAMES)
+
+
+class LimParams(C.Structure):
+    """lim_params: every field 8 bytes wide (same layout in C, Julia and here)."""
+    _fields_ = [(n, C.c_double) for n in ("dt", "t0", "m", "DsT", "Tfo", "psi2", "obs_pt_cut", "obs_pt_width")] + \
+               [(n, C.c_int64) for n in ("dims", "pdim", "coords", "collision", "relativistic", "bjorken_redshift",
+                                         "position_diffusion", "reflecting_boundary", "integrator_mode",
+                                         "freezeout_capture", "freezeout_interp", "precision", "seed",
+                                         "particle_offset", "stop_after_freezeout", "block_size")]
+
+
+class LimError(RuntimeError):
+    """A non-zero status from the engine; ``code`` is the LIM_ERR_* value."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+_lib = None
+
+_DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
+_U32P = C.POINTER(C.c_uint32)
+_I64P = C.POINTER(C.c_int64)
+
+_SIGS = {
+    "lim_abi_version": ([], C.c_int),
+    "lim_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "lim_destroy": ([C.c_void_p], C.c_int),
+    "lim_last_error": ([C.c_void_p], C.c_char_p),
+    "lim_synchronize": ([C.c_void_p], C.c_int),
+    "lim_device_bytes": ([C.c_void_p, _I64P], C.c_int),
+    "lim_set_params": ([C.c_void_p, C.POINTER(LimParams)], C.c_int),
+    "lim_set_medium_rt": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, _DP, _DP, _DP], C.c_int),
+    "lim_set_medium_bjorken": ([C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double], C.c_int),
+    "lim_set_medium_grid": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
+                             C.c_double, C.c_double, C.c_double, _FP, _FP, _FP], C.c_int),
+    "lim_set_spline": ([C.c_void_p, C.c_int, C.c_double, C.c_double, _DP, C.c_int64], C.c_int),
+    "lim_set_invcdf": ([C.c_void_p, _DP, C.c_int64, C.c_int64, C.c_double, C.c_double], C.c_int),
+    "lim_upload_state": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, C.c_int64], C.c_int),
+    "lim_download_state": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_initial_lab_boost": ([C.c_void_p], C.c_int),
+    "lim_run": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
+    "lim_status": ([C.c_void_p, _I64P], C.c_int),
+    "lim_download_freezeout": ([C.c_void_p, _DP, _DP, _DP, _DP], C.c_int),
+    "lim_observables": ([C.c_void_p, C.c_int, _DP], C.c_int),
+    "lim_record_noise": ([C.c_void_p, C.c_int64, C.c_int64], C.c_int),
+    "lim_download_noise": ([C.c_void_p, _DP], C.c_int),
+    "lim_philox_device": ([C.c_void_p, _U32P, _U32P, _U32P], C.c_int),
+    "lim_last_run_stats": ([C.c_void_p, _DP, _I64P], C.c_int),
+}
+
+
+def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the engine.  Raises if the in-tree library has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with __graft_entry__.build() "
+                          "(there is no CPU fallback for the engine)")
+    lib = C.CDLL(str(p))
+    for name, (args, res) in _SIGS.items():
+        if hasattr(lib, name):
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_DP)
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
+
+
+def julia_layout(a, rows: int) -> np.ndarray:
+    """(rows, N) array -> the column-major flat buffer a Julia Matrix would hold."""
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        a = a.reshape(1, -1)
+    if a.shape[0] != rows:
+        raise ValueError(f"expected {rows} rows, got array of shape {a.shape}")
+    return np.ascontiguousarray(a.T).reshape(-1)
+
+
+def from_julia_layout(buf: np.ndarray, rows: int, n: int) -> np.ndarray:
+    """Flat column-major buffer -> (rows, N) array view."""
+    return buf.reshape(n, rows).T
+
+
+class Engine:
+    """One engine context on one CUDA device (lim_create .. lim_destroy)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None, lib: C.CDLL | None = None):
+        self.lib = lib or load_library()
+        self.ctx = C.c_void_p()
+        rc = self.lib.lim_create(int(device), C.c_void_p(stream) if stream else None, C.byref(self.ctx))
+        if rc != LIM_OK:
+            raise LimError(rc, self.lib.lim_last_error(None).decode())
+        self.params = LimParams()
+        self.n = 0
+
+    # -- plumbing ------------------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != LIM_OK:
+            raise LimError(rc, self.lib.lim_last_error(self.ctx).decode())
+
+    def close(self):
+        if self.ctx:
+            self.lib.lim_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- configuration ---------------------------------------------------------------
+    def set_params(self, **kw):
+        P = LimParams()
+        defaults = dict(dt=0.001, t0=0.0, m=1.0, DsT=0.2, Tfo=0.156, psi2=0.0, obs_pt_cut=5.0, obs_pt_width=0.1,
+                        dims=3, pdim=0, coords=0, collision=0, relativistic=1, bjorken_redshift=0,
+                        position_diffusion=0, reflecting_boundary=0, integrator_mode=0, freezeout_capture=0,
+                        freezeout_interp=1, precision=0, seed=0x4C494D00, particle_offset=0,
+                        stop_after_freezeout=0, block_size=0)
+        unknown = set(kw) - set(defaults)
+        if unknown:
+            raise TypeError(f"unknown engine parameters: {sorted(unknown)}")
+        defaults.update(kw)
+        for k, v in defaults.items():
+            setattr(P, k, float(v) if isinstance(getattr(P, k), float) else int(v))
+        self._check(self.lib.lim_set_params(self.ctx, C.byref(P)))
+        self.params = P
+        if P.pdim <= 0:
+            P.pdim = P.dims
+        return P
+
+    def set_medium_rt(self, xgrid, tgrid, T, V, V2=None):
+        xg = np.ascontiguousarray(xgrid, dtype=np.float64)
+        tg = np.ascontiguousarray(tgrid, dtype=np.float64)
+        Tf = np.ascontiguousarray(np.asarray(T, dtype=np.float64).ravel(order="F"))
+        Vf = np.ascontiguousarray(np.asarray(V, dtype=np.float64).ravel(order="F"))
+        V2f = None if V2 is None else np.ascontiguousarray(np.asarray(V2, dtype=np.float64).ravel(order="F"))
+        if Tf.size != xg.size * tg.size or Vf.size != Tf.size or (V2f is not None and V2f.size != Tf.size):
+            raise ValueError("T/V/V2 must have shape (len(xgrid), len(tgrid))")
+        self._check(self.lib.lim_set_medium_rt(self.ctx, _dptr(xg), xg.size, _dptr(tg), tg.size,
+                                               _dptr(Tf), _dptr(Vf), _dptr(V2f)))
+
+    def set_medium_bjorken(self, T0, tau0, power=1.0 / 3.0, r_max=0.0):
+        self._check(self.lib.lim_set_medium_bjorken(self.ctx, T0, tau0, power, r_max))
+
+    def set_medium_grid(self, T, ux, uy, x0, dx, y0, dy, tau0, dtau):
+        """Fields of shape (nt, ny, nx) (x fastest)."""
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        ux = np.ascontiguousarray(ux, dtype=np.float32)
+        uy = np.ascontiguousarray(uy, dtype=np.float32)
+        nt, ny, nx = T.shape
+        if ux.shape != T.shape or uy.shape != T.shape:
+            raise ValueError("T, ux, uy must share the shape (nt, ny, nx)")
+        self._check(self.lib.lim_set_medium_grid(self.ctx, nx, ny, nt, x0, dx, y0, dy, tau0, dtau,
+                                                 _fptr(T), _fptr(ux), _fptr(uy)))
+
+    def set_spline(self, which, Tmin, invdT, vals):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        self._check(self.lib.lim_set_spline(self.ctx, int(which), float(Tmin), float(invdT), _dptr(v), v.size))
+
+    def set_invcdf(self, vals, nU, nT, Tmin, invdT):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        self._check(self.lib.lim_set_invcdf(self.ctx, _dptr(v), int(nU), int(nT), float(Tmin), float(invdT)))
+
+    # -- state -----------------------------------------------------------------------
+    def upload_state(self, x, p):
+        dims, pdim = int(self.params.dims), int(self.params.pdim)
+        xb = julia_layout(x, dims)
+        pb = julia_layout(p, pdim)
+        n = xb.size // dims
+        if pb.size != n * pdim:
+            raise ValueError("x and p hold different particle counts")
+        self._check(self.lib.lim_upload_state(self.ctx, _dptr(xb), dims, _dptr(pb), pdim, n))
+        self.n = n
+
+    def upload_state_flat(self, xbuf: np.ndarray, pbuf: np.ndarray, n: int):
+        """Upload from flat Julia-layout buffers (e.g. pinned host memory)."""
+        self._check(self.lib.lim_upload_state(self.ctx, _dptr(xbuf), int(self.params.dims), _dptr(pbuf),
+                                              int(self.params.pdim), int(n)))
+        self.n = int(n)
+
+    def download_state(self):
+        dims, pdim, n = int(self.params.dims), int(self.params.pdim), self.n
+        xb = np.empty(max(n * dims, 1))
+        pb = np.empty(max(n * pdim, 1))
+        self._check(self.lib.lim_download_state(self.ctx, _dptr(xb), _dptr(pb)))
+        return from_julia_layout(xb[:n * dims], dims, n), from_julia_layout(pb[:n * pdim], pdim, n)
+
+    def download_state_flat(self, xbuf: np.ndarray | None, pbuf: np.ndarray | None):
+        self._check(self.lib.lim_download_state(self.ctx, _dptr(xbuf), _dptr(pbuf)))
+
+    def initial_lab_boost(self):
+        self._check(self.lib.lim_initial_lab_boost(self.ctx))
+
+    def run(self, first_step: int, nsteps: int, save_every: int = 0, first_slot: int = 0,
+            hist_x: np.ndarray | None = None, hist_p: np.ndarray | None = None):
+        self._check(self.lib.lim_run(self.ctx, int(first_step), int(nsteps), int(save_every), int(first_slot),
+                                     _dptr(hist_x), _dptr(hist_p)))
+
+    def status(self) -> int:
+        v = C.c_int64(-1)
+        self._check(self.lib.lim_status(self.ctx, C.byref(v)))
+        return int(v.value)
+
+    def download_freezeout(self):
+        dims, pdim, n = int(self.params.dims), int(self.params.pdim), self.n
+        fp, fm, ft, ff = np.empty(max(n * dims, 1)), np.empty(max(n * pdim, 1)), np.empty(max(n, 1)), np.empty(max(n, 1))
+        self._check(self.lib.lim_download_freezeout(self.ctx, _dptr(fp), _dptr(fm), _dptr(ft), _dptr(ff)))
+        return dict(pos=from_julia_layout(fp[:n * dims], dims, n), mom=from_julia_layout(fm[:n * pdim], pdim, n),
+                    tau=ft[:n].copy(), flag=ff[:n].copy())
+
+    def observables(self, from_freezeout: bool = False) -> dict:
+        out = np.zeros(LIM_OBS_NUM)
+        self._check(self.lib.lim_observables(self.ctx, int(bool(from_freezeout)), _dptr(out)))
+        cnt = out[0]
+        res = {"count": cnt}
+        for k, name in enumerate(OBS_NAMES[1:], start=1):
+            res[name] = out[k] / cnt if cnt > 0 else float("nan")
+        res["sums"] = out
+        return res
+
+    def record_noise(self, first_step: int, nsteps: int):
+        self._check(self.lib.lim_record_noise(self.ctx, int(first_step), int(nsteps)))
+        self._rec_steps = int(nsteps)
+
+    def download_noise(self) -> np.ndarray:
+        out = np.empty(self._rec_steps * LIM_NOISE_SLOTS * self.n)
+        self._check(self.lib.lim_download_noise(self.ctx, _dptr(out)))
+        return out.reshape(self._rec_steps, LIM_NOISE_SLOTS, self.n)
+
+    def philox(self, ctr, key):
+        c = (C.c_uint32 * 4)(*ctr)
+        k = (C.c_uint32 * 2)(*key)
+        o = (C.c_uint32 * 4)()
+        self._check(self.lib.lim_philox_device(self.ctx, c, k, o))
+        return list(o)
+
+    def last_run_stats(self):
+        ms = C.c_double(0.0)
+        nl = C.c_int64(0)
+        self._check(self.lib.lim_last_run_stats(self.ctx, C.byref(ms), C.byref(nl)))
+        return ms.value, int(nl.value)
+
+    def device_bytes(self) -> int:
+        v = C.c_int64(0)
+        self._check(self.lib.lim_device_bytes(self.ctx, C.byref(v)))
+        return int(v.value)
+
+    def synchronize(self):
+        self._check(self.lib.lim_synchronize(self.ctx))

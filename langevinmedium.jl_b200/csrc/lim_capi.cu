@@ -1,0 +1,811 @@
+// lim_capi.cu — the C-ABI (include/langevin_b200.h) over the fused step kernels.
+//
+// Validation mirrors the reference's errors (check_momentum_dims, utils.jl:561-573;
+// collision_mode, simulate_gpu_wrapper.jl:54-55; spline range, transport.jl:182-184).
+// No exception crosses the ABI: every entry point returns a status and keeps the
+// message for lim_last_error().
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <climits>
+#include <new>
+#include <string>
+#include <vector>
+#include "../../include/langevin_b200.h"
+#include "lim_internal.h"
+
+using namespace lim;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct lim_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+
+    lim_params P{};
+    bool have_params = false;
+
+    // host copy of the medium
+    int med_kind = -1;
+    std::vector<double> xg, tg, T, V, V2;
+    double bj_T0 = 0, bj_tau0 = 0, bj_power = 0, bj_rmax = 0;
+    int64_t gnx = 0, gny = 0, gnt = 0;
+    double gx0 = 0, gdx = 0, gy0 = 0, gdy = 0, gt0 = 0, gdt = 0;
+    std::vector<float> gT, gux, guy;
+    std::vector<double> spl[2];
+    double spl_Tmin[2] = { 0, 0 }, spl_invdT[2] = { 1, 1 };
+    std::vector<double> icdf;
+    int64_t nU = 0, nT = 0;
+    double ic_Tmin = 0, ic_invdT = 1;
+    double T_scale = 1.0;
+
+    // device copy of the medium for `dev_prec`
+    int dev_prec = -1;
+    bool dev_dirty = true;
+    DevBuf d_xg, d_tg, d_tgd, d_TV, d_V2, d_G, d_spl[2], d_icdf;
+
+    // particle state (structure of arrays, precision `state_prec`)
+    int64_t n = 0;
+    int dims = 0, pdim = 0, state_prec = -1;
+    bool have_state = false;
+    DevBuf d_x[3], d_xlo[3], d_p[3];
+    DevBuf d_fo_pos[3], d_fo_mom[3], d_fo_tau, d_fo_flag, d_l_pos[3], d_l_mom[3], d_l_tau, d_l_T;
+    DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe;
+    DevBuf d_rec;
+    int64_t rec_first = 0, rec_steps = 0;
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+};
+
+namespace {
+
+int fail(lim_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf; else g_create_error = buf;
+    return code;
+}
+
+#define LIM_CUDA(ctx, call)                                                                     \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail((ctx), LIM_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));   \
+    } while (0)
+
+int dev_alloc(lim_ctx* c, DevBuf& b, size_t bytes)
+{
+    if (b.bytes >= bytes && b.p) return LIM_OK;
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+    if (bytes == 0) return LIM_OK;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return fail(c, LIM_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return LIM_OK;
+}
+void dev_free(DevBuf& b)
+{
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+template <typename T>
+int upload(lim_ctx* c, DevBuf& b, const T* src, size_t count)
+{
+    int rc = dev_alloc(c, b, count * sizeof(T));
+    if (rc) return rc;
+    if (count) LIM_CUDA(c, cudaMemcpyAsync(b.p, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));   // the host vectors may be released afterwards
+    return LIM_OK;
+}
+
+bool all_finite(const double* v, size_t n)
+{
+    for (size_t i = 0; i < n; ++i) if (!std::isfinite(v[i])) return false;
+    return true;
+}
+bool ascending(const double* v, size_t n)
+{
+    for (size_t i = 1; i < n; ++i) if (!(v[i] > v[i - 1])) return false;
+    return true;
+}
+// A grid is "uniform" when node k lies within half a spacing of x0 + k h: the
+// O(1) guess of the cell search then needs at most one correction step.
+bool near_uniform(const std::vector<double>& g, double& x0, double& inv)
+{
+    size_t n = g.size();
+    x0 = g[0];
+    double h = (g[n - 1] - g[0]) / (double)(n - 1);
+    inv = h > 0 ? 1.0 / h : 0.0;
+    if (!(h > 0)) return false;
+    for (size_t k = 0; k < n; ++k)
+        if (std::fabs(g[k] - (x0 + (double)k * h)) > 0.5 * h) return false;
+    return true;
+}
+
+int state_rows_ok(lim_ctx* c)
+{
+    if (!c->have_params) return fail(c, LIM_ERR_STATE, "lim_set_params must be called first");
+    return LIM_OK;
+}
+
+template <typename R>
+int ensure_device_medium(lim_ctx* c)
+{
+    const int prec = sizeof(R) == 8 ? LIM_FP64 : LIM_FP32;
+    if (!c->dev_dirty && c->dev_prec == prec) return LIM_OK;
+    int rc;
+    if (c->med_kind == MED_RT) {
+        size_t nr = c->xg.size(), nt = c->tg.size();
+        std::vector<R> xr(nr), tr(nt);
+        for (size_t k = 0; k < nr; ++k) xr[k] = (R)c->xg[k];
+        for (size_t k = 0; k < nt; ++k) tr[k] = (R)c->tg[k];
+        std::vector<R> tv(2 * nr * nt);
+        for (size_t k = 0; k < nr * nt; ++k) { tv[2 * k] = (R)c->T[k]; tv[2 * k + 1] = (R)c->V[k]; }
+        if ((rc = upload(c, c->d_xg, xr.data(), nr))) return rc;
+        if ((rc = upload(c, c->d_tg, tr.data(), nt))) return rc;
+        if ((rc = upload(c, c->d_tgd, c->tg.data(), nt))) return rc;
+        if ((rc = upload(c, c->d_TV, tv.data(), tv.size()))) return rc;
+        if (!c->V2.empty()) {
+            std::vector<R> v2(c->V2.size());
+            for (size_t k = 0; k < v2.size(); ++k) v2[k] = (R)c->V2[k];
+            if ((rc = upload(c, c->d_V2, v2.data(), v2.size()))) return rc;
+        }
+    } else if (c->med_kind == MED_GRID) {
+        size_t nn = (size_t)(c->gnx * c->gny * c->gnt);
+        std::vector<float4> g(nn);
+        for (size_t k = 0; k < nn; ++k) g[k] = make_float4(c->gT[k], c->gux[k], c->guy[k], 0.f);
+        if ((rc = upload(c, c->d_G, g.data(), nn))) return rc;
+    }
+    for (int w = 0; w < 2; ++w) {
+        if (c->spl[w].empty()) continue;
+        std::vector<R> s(c->spl[w].size());
+        for (size_t k = 0; k < s.size(); ++k) s[k] = (R)c->spl[w][k];
+        if ((rc = upload(c, c->d_spl[w], s.data(), s.size()))) return rc;
+    }
+    if (!c->icdf.empty()) {
+        std::vector<R> s(c->icdf.size());
+        for (size_t k = 0; k < s.size(); ++k) s[k] = (R)c->icdf[k];
+        if ((rc = upload(c, c->d_icdf, s.data(), s.size()))) return rc;
+    }
+    c->dev_prec = prec;
+    c->dev_dirty = false;
+    return LIM_OK;
+}
+
+template <typename R>
+int build_kparams(lim_ctx* c, KParams<R>& kp)
+{
+    int rc = ensure_device_medium<R>(c);
+    if (rc) return rc;
+    std::memset(&kp, 0, sizeof kp);
+    const lim_params& P = c->P;
+    kp.dt = P.dt; kp.t0 = P.t0;
+    kp.m = (R)P.m; kp.DsT = (R)P.DsT; kp.Tfo = (R)P.Tfo; kp.psi2 = (R)P.psi2;
+    kp.sqrt_dt = (R)std::sqrt(P.dt); kp.dtR = (R)P.dt;
+    kp.rel = P.relativistic != 0; kp.collision = (int)P.collision; kp.redshift = P.bjorken_redshift != 0;
+    kp.diffusion = P.position_diffusion != 0; kp.reflect = P.reflecting_boundary != 0;
+    kp.integrator = (int)P.integrator_mode; kp.fo_capture = P.freezeout_capture != 0;
+    kp.fo_interp = P.freezeout_interp != 0; kp.stop_fo = P.stop_after_freezeout != 0 && P.freezeout_capture != 0;
+    kp.seed_lo = (uint32_t)(uint64_t)P.seed; kp.seed_hi = (uint32_t)((uint64_t)P.seed >> 32);
+    kp.pid_offset = P.particle_offset;
+    kp.n = c->n; kp.dims = c->dims; kp.pdim = c->pdim;
+    kp.drag = (const R*)c->d_spl[0].p; kp.n_drag = (int)c->spl[0].size();
+    kp.drag_Tmin = (R)c->spl_Tmin[0]; kp.drag_invdT = (R)c->spl_invdT[0];
+    kp.rta = (const R*)c->d_spl[1].p; kp.n_rta = (int)c->spl[1].size();
+    kp.rta_Tmin = (R)c->spl_Tmin[1]; kp.rta_invdT = (R)c->spl_invdT[1];
+    kp.icdf = (const R*)c->d_icdf.p; kp.nU = (int)c->nU; kp.nT = (int)c->nT;
+    kp.ic_Tmin = (R)c->ic_Tmin; kp.ic_invdT = (R)c->ic_invdT;
+    MediumDev<R>& md = kp.med;
+    md.kind = c->med_kind;
+    md.T_scale = (R)c->T_scale;
+    if (c->med_kind == MED_RT) {
+        md.xg = (const R*)c->d_xg.p; md.tg = (const R*)c->d_tg.p; md.tgd = (const double*)c->d_tgd.p;
+        md.nr = (int)c->xg.size(); md.nt = (int)c->tg.size();
+        double x0, xi, t0g, ti;
+        md.x_uniform = near_uniform(c->xg, x0, xi); md.xg0 = (R)x0; md.xinvd = (R)xi;
+        md.t_uniform = near_uniform(c->tg, t0g, ti); md.tg0 = t0g; md.tinvd = ti;
+        md.TV = (const typename V2T<R>::type*)c->d_TV.p;
+        md.V2 = (const R*)c->d_V2.p; md.use_v2 = !c->V2.empty();
+        md.r_max = (R)c->xg.back();
+        md.r_axis_eps = (R)std::max(1e-12, 0.5 * std::fabs(c->xg[1] - c->xg[0]));
+    } else if (c->med_kind == MED_BJORKEN) {
+        md.bj_T0 = c->bj_T0; md.bj_tau0 = c->bj_tau0; md.bj_power = c->bj_power;
+        md.r_max = (R)c->bj_rmax; md.r_axis_eps = (R)1e-6;
+    } else {
+        md.G = (const float4*)c->d_G.p;
+        md.gnx = (int)c->gnx; md.gny = (int)c->gny; md.gnt = (int)c->gnt;
+        md.gx0_d = c->gx0; md.gdx_d = c->gdx; md.gxl_d = c->gx0 + (double)(c->gnx - 1) * c->gdx;
+        md.gy0_d = c->gy0; md.gdy_d = c->gdy; md.gyl_d = c->gy0 + (double)(c->gny - 1) * c->gdy;
+        md.ginvdx = (float)(1.0 / c->gdx); md.ginvdy = (float)(1.0 / c->gdy);
+        md.gt0 = c->gt0; md.gdt_d = c->gdt; md.gtl = c->gt0 + (double)(c->gnt - 1) * c->gdt;
+        double r = std::fabs(md.gx0_d);
+        r = std::min(r, std::fabs(md.gxl_d)); r = std::min(r, std::fabs(md.gy0_d)); r = std::min(r, std::fabs(md.gyl_d));
+        md.r_max = (R)r; md.r_axis_eps = (R)1e-6;
+    }
+    for (int d = 0; d < 3; ++d) {
+        kp.x[d] = (R*)c->d_x[d].p; kp.xlo[d] = (float*)c->d_xlo[d].p; kp.p[d] = (R*)c->d_p[d].p;
+        kp.fo_pos[d] = (R*)c->d_fo_pos[d].p; kp.fo_mom[d] = (R*)c->d_fo_mom[d].p;
+        kp.l_pos[d] = (R*)c->d_l_pos[d].p; kp.l_mom[d] = (R*)c->d_l_mom[d].p;
+    }
+    kp.fo_tau = (R*)c->d_fo_tau.p; kp.fo_flag = (R*)c->d_fo_flag.p;
+    kp.l_tau = (R*)c->d_l_tau.p; kp.l_T = (R*)c->d_l_T.p;
+    kp.first_bad = (unsigned long long*)c->d_status.p;
+    kp.rec = (double*)c->d_rec.p; kp.rec_first = c->rec_first; kp.rec_steps = c->d_rec.p ? c->rec_steps : 0;
+    return LIM_OK;
+}
+
+int check_ready(lim_ctx* c)
+{
+    if (!c->have_params) return fail(c, LIM_ERR_STATE, "lim_set_params must be called before running");
+    if (c->med_kind < 0) return fail(c, LIM_ERR_STATE, "no medium set (lim_set_medium_rt/_bjorken/_grid)");
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "no particle state uploaded (lim_upload_state)");
+    if (c->P.coords == LIM_COORDS_MILNE && c->med_kind != MED_RT)
+        return fail(c, LIM_ERR_UNSUPPORTED, "Milne (tau, r) coordinates need the (r, t) table medium");
+    if (c->med_kind == MED_GRID && c->dims != 2)
+        return fail(c, LIM_ERR_UNSUPPORTED, "the 2+1D grid medium needs dimensions=2 (got %d)", c->dims);
+    const int coll = (int)c->P.collision;
+    const bool langevin = coll == LIM_COLL_LANGEVIN || coll == LIM_COLL_LANGEVIN_RTA || c->P.coords == LIM_COORDS_MILNE;
+    const bool rta = coll == LIM_COLL_RTA || coll == LIM_COLL_LANGEVIN_RTA;
+    if (langevin && c->P.DsT > 0 && c->spl[0].empty())
+        return fail(c, LIM_ERR_STATE, "drag spline not set (lim_set_spline LIM_SPLINE_DRAG) but DsT > 0");
+    if (rta && c->P.coords != LIM_COORDS_MILNE) {
+        if (c->P.DsT > 0 && c->spl[1].empty())
+            return fail(c, LIM_ERR_STATE, "RTA spline not set (lim_set_spline LIM_SPLINE_RTA)");
+        if (c->icdf.empty()) return fail(c, LIM_ERR_STATE, "RTA needs the Juttner inverse CDF (lim_set_invcdf)");
+    }
+    if (c->state_prec != (int)c->P.precision)
+        return fail(c, LIM_ERR_STATE, "state was uploaded in another precision; upload it again");
+    return LIM_OK;
+}
+
+int block_of(const lim_ctx* c)
+{
+    int b = (int)c->P.block_size;
+    if (b <= 0) b = 256;
+    return b;
+}
+
+template <typename R>
+int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
+             double* hist_x, double* hist_p)
+{
+    KParams<R> kp;
+    int rc = build_kparams<R>(c, kp);
+    if (rc) return rc;
+    const int block = block_of(c);
+    const bool saving = save_every > 0 && (hist_x || hist_p);
+    const int64_t end = first_step + nsteps;
+    int64_t launches = 0;
+    LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int64_t s = first_step;
+    while (s < end) {
+        int64_t chunk_end = end;
+        if (saving) {   // run through the next save step (inclusive), then snapshot
+            const int64_t next_save = ((s + save_every - 1) / save_every) * save_every;   // s >= 0
+            if (next_save + 1 < chunk_end) chunk_end = next_save + 1;
+        }
+        LIM_CUDA(c, launch_steps<R>(kp, (int)c->P.coords, s, chunk_end, block, c->stream));
+        ++launches;
+        const int64_t last = chunk_end - 1;
+        if (saving && last % save_every == 0 && last >= 0) {
+            const int64_t slot = last / save_every - first_slot;
+            if (slot >= 0) {
+                R* xs[3] = { kp.x[0], kp.x[1], kp.x[2] };
+                R* ps[3] = { kp.p[0], kp.p[1], kp.p[2] };
+                if (hist_x) {
+                    LIM_CUDA(c, launch_soa_to_aos<R>(xs, sizeof(R) == 4 ? kp.xlo : nullptr, c->dims, c->n,
+                                                     (double*)c->d_stage_x.p, c->stream));
+                    LIM_CUDA(c, cudaMemcpyAsync(hist_x + slot * c->n * c->dims, c->d_stage_x.p,
+                                                sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
+                }
+                if (hist_p) {
+                    LIM_CUDA(c, launch_soa_to_aos<R>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+                    LIM_CUDA(c, cudaMemcpyAsync(hist_p + slot * c->n * c->pdim, c->d_stage_p.p,
+                                                sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
+                }
+                launches += 2;
+            }
+        }
+        s = chunk_end;
+    }
+    LIM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    LIM_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    LIM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    c->last_launches = launches;
+    unsigned long long bad = ULLONG_MAX;
+    LIM_CUDA(c, cudaMemcpy(&bad, c->d_status.p, sizeof bad, cudaMemcpyDeviceToHost));
+    if (bad != ULLONG_MAX)
+        return fail(c, LIM_ERR_NONFINITE, "Breaking simulation due to NaN/Inf at step %llu", bad);
+    return LIM_OK;
+}
+
+template <typename R>
+int alloc_state(lim_ctx* c, int64_t n)
+{
+    int rc;
+    const size_t nb = (size_t)n * sizeof(R);
+    for (int d = 0; d < 3; ++d) {
+        dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
+        dev_free(c->d_fo_pos[d]); dev_free(c->d_fo_mom[d]); dev_free(c->d_l_pos[d]); dev_free(c->d_l_mom[d]);
+    }
+    dev_free(c->d_fo_tau); dev_free(c->d_fo_flag); dev_free(c->d_l_tau); dev_free(c->d_l_T);
+    if (n == 0) return LIM_OK;
+    for (int d = 0; d < c->dims; ++d) {
+        if ((rc = dev_alloc(c, c->d_x[d], nb))) return rc;
+        if (sizeof(R) == 4 && (rc = dev_alloc(c, c->d_xlo[d], (size_t)n * sizeof(float)))) return rc;
+    }
+    for (int d = 0; d < c->pdim; ++d)
+        if ((rc = dev_alloc(c, c->d_p[d], nb))) return rc;
+    if (c->P.freezeout_capture) {
+        for (int d = 0; d < c->dims; ++d) {
+            if ((rc = dev_alloc(c, c->d_fo_pos[d], nb))) return rc;
+            if ((rc = dev_alloc(c, c->d_l_pos[d], nb))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_pos[d].p, 0, nb, c->stream));
+            LIM_CUDA(c, cudaMemsetAsync(c->d_l_pos[d].p, 0, nb, c->stream));
+        }
+        for (int d = 0; d < c->pdim; ++d) {
+            if ((rc = dev_alloc(c, c->d_fo_mom[d], nb))) return rc;
+            if ((rc = dev_alloc(c, c->d_l_mom[d], nb))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_mom[d].p, 0, nb, c->stream));
+            LIM_CUDA(c, cudaMemsetAsync(c->d_l_mom[d].p, 0, nb, c->stream));
+        }
+        DevBuf* bufs[4] = { &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T };
+        for (DevBuf* b : bufs) {
+            if ((rc = dev_alloc(c, *b, nb))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(b->p, 0, nb, c->stream));
+        }
+    }
+    return LIM_OK;
+}
+
+template <typename R>
+int upload_state_impl(lim_ctx* c, const double* x, const double* p, int64_t n)
+{
+    int rc;
+    if ((rc = alloc_state<R>(c, n))) return rc;
+    if ((rc = dev_alloc(c, c->d_stage_x, (size_t)std::max<int64_t>(n, 1) * c->dims * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_stage_p, (size_t)std::max<int64_t>(n, 1) * c->pdim * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_status, sizeof(unsigned long long)))) return rc;
+    LIM_CUDA(c, cudaMemsetAsync(c->d_status.p, 0xff, sizeof(unsigned long long), c->stream));
+    c->n = n;
+    if (n > 0) {
+        LIM_CUDA(c, cudaMemcpyAsync(c->d_stage_x.p, x, sizeof(double) * n * c->dims, cudaMemcpyHostToDevice, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(c->d_stage_p.p, p, sizeof(double) * n * c->pdim, cudaMemcpyHostToDevice, c->stream));
+        R* xs[3] = { (R*)c->d_x[0].p, (R*)c->d_x[1].p, (R*)c->d_x[2].p };
+        R* ps[3] = { (R*)c->d_p[0].p, (R*)c->d_p[1].p, (R*)c->d_p[2].p };
+        float* lo[3] = { (float*)c->d_xlo[0].p, (float*)c->d_xlo[1].p, (float*)c->d_xlo[2].p };
+        LIM_CUDA(c, launch_aos_to_soa<R>((const double*)c->d_stage_x.p, c->dims, n, xs, sizeof(R) == 4 ? lo : nullptr, c->stream));
+        LIM_CUDA(c, launch_aos_to_soa<R>((const double*)c->d_stage_p.p, c->pdim, n, ps, nullptr, c->stream));
+    }
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->state_prec = (int)c->P.precision;
+    c->have_state = true;
+    return LIM_OK;
+}
+
+template <typename R>
+int download_state_impl(lim_ctx* c, double* x, double* p)
+{
+    if (c->n == 0) return LIM_OK;
+    R* xs[3] = { (R*)c->d_x[0].p, (R*)c->d_x[1].p, (R*)c->d_x[2].p };
+    R* ps[3] = { (R*)c->d_p[0].p, (R*)c->d_p[1].p, (R*)c->d_p[2].p };
+    float* lo[3] = { (float*)c->d_xlo[0].p, (float*)c->d_xlo[1].p, (float*)c->d_xlo[2].p };
+    if (x) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(xs, sizeof(R) == 4 ? lo : nullptr, c->dims, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(x, c->d_stage_x.p, sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (p) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(p, c->d_stage_p.p, sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
+    }
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+template <typename R>
+int download_fo_impl(lim_ctx* c, double* fo_pos, double* fo_mom, double* fo_tau, double* fo_flag)
+{
+    if (!c->P.freezeout_capture) return fail(c, LIM_ERR_STATE, "freezeout_capture is off");
+    if (c->n == 0) return LIM_OK;
+    R* fp[3] = { (R*)c->d_fo_pos[0].p, (R*)c->d_fo_pos[1].p, (R*)c->d_fo_pos[2].p };
+    R* fm[3] = { (R*)c->d_fo_mom[0].p, (R*)c->d_fo_mom[1].p, (R*)c->d_fo_mom[2].p };
+    R* ft[1] = { (R*)c->d_fo_tau.p };
+    R* ff[1] = { (R*)c->d_fo_flag.p };
+    if (fo_pos) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(fp, nullptr, c->dims, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(fo_pos, c->d_stage_x.p, sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (fo_mom) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(fm, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(fo_mom, c->d_stage_p.p, sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
+    }
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (fo_tau) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(ft, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(fo_tau, c->d_stage_x.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    if (fo_flag) {
+        LIM_CUDA(c, launch_soa_to_aos<R>(ff, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, cudaMemcpyAsync(fo_flag, c->d_stage_x.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    return LIM_OK;
+}
+
+template <typename R>
+int observables_impl(lim_ctx* c, int from_fo, double* out)
+{
+    KParams<R> kp;
+    int rc = build_kparams<R>(c, kp);
+    if (rc) return rc;
+    if (from_fo && !c->P.freezeout_capture) return fail(c, LIM_ERR_STATE, "freezeout_capture is off");
+    const int64_t nb = c->n == 0 ? 1 : (c->n + 255) / 256;
+    if ((rc = dev_alloc(c, c->d_partials, (size_t)nb * kObsNum * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_obs, kObsNum * sizeof(double)))) return rc;
+    LIM_CUDA(c, launch_observables<R>(kp, from_fo, c->P.obs_pt_cut, c->P.obs_pt_width > 0 ? c->P.obs_pt_width : 1e-3,
+                                      (double*)c->d_partials.p, nb, (double*)c->d_obs.p, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync(out, c->d_obs.p, kObsNum * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+int lim_abi_version(void) { return LIM_ABI_VERSION; }
+
+int lim_create(int device, void* stream, lim_ctx** out)
+{
+    if (!out) return fail(nullptr, LIM_ERR_ARG, "lim_create: out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess) return fail(nullptr, LIM_ERR_CUDA, "cudaGetDeviceCount failed: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(nullptr, LIM_ERR_ARG, "lim_create: device %d out of range (%d devices)", device, ndev);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, LIM_ERR_CUDA, "cudaSetDevice failed: %s", cudaGetErrorString(e));
+    lim_ctx* c = new (std::nothrow) lim_ctx();
+    if (!c) return fail(nullptr, LIM_ERR_NOMEM, "lim_create: out of host memory");
+    c->device = device;
+    if (stream) c->stream = (cudaStream_t)stream;
+    else {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete c; return fail(nullptr, LIM_ERR_CUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e)); }
+        c->own_stream = true;
+    }
+    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return fail(nullptr, LIM_ERR_CUDA, "cudaEventCreate failed");
+    }
+    *out = c;
+    return LIM_OK;
+}
+
+int lim_destroy(lim_ctx* c)
+{
+    if (!c) return LIM_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+                      &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
+                      &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec };
+    for (DevBuf* b : all) dev_free(*b);
+    for (int d = 0; d < 3; ++d) {
+        dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
+        dev_free(c->d_fo_pos[d]); dev_free(c->d_fo_mom[d]); dev_free(c->d_l_pos[d]); dev_free(c->d_l_mom[d]);
+    }
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return LIM_OK;
+}
+
+const char* lim_last_error(const lim_ctx* c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+int lim_synchronize(lim_ctx* c)
+{
+    if (!c) return LIM_ERR_ARG;
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
+{
+    if (!c || !bytes) return LIM_ERR_ARG;
+    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+                            &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
+                            &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec };
+    int64_t t = 0;
+    for (const DevBuf* b : all) t += (int64_t)b->bytes;
+    for (int d = 0; d < 3; ++d)
+        t += (int64_t)(c->d_x[d].bytes + c->d_xlo[d].bytes + c->d_p[d].bytes + c->d_fo_pos[d].bytes +
+                       c->d_fo_mom[d].bytes + c->d_l_pos[d].bytes + c->d_l_mom[d].bytes);
+    *bytes = t;
+    return LIM_OK;
+}
+
+int lim_set_params(lim_ctx* c, const lim_params* P)
+{
+    if (!c || !P) return LIM_ERR_ARG;
+    lim_params q = *P;
+    if (!std::isfinite(q.dt) || !std::isfinite(q.t0) || !std::isfinite(q.m))
+        return fail(c, LIM_ERR_ARG, "dt, t0 and m must be finite");
+    if (q.pdim <= 0) q.pdim = q.dims;                          // momentum_dimensions = 0 => dimensions
+    if (q.coords != LIM_COORDS_CARTESIAN && q.coords != LIM_COORDS_MILNE)
+        return fail(c, LIM_ERR_ARG, "coords=%lld is not a valid coordinate system", (long long)q.coords);
+    if (q.coords == LIM_COORDS_MILNE) {
+        if (q.dims != 2 || q.pdim != 2)
+            return fail(c, LIM_ERR_ARG, "Milne coordinates evolve (tau, r) and (p^tau, p^r): dims = pdim = 2");
+    } else {
+        if (q.dims < 1 || q.dims > 3) return fail(c, LIM_ERR_ARG, "dimensions=%lld is not supported (1, 2 or 3)", (long long)q.dims);
+        const bool radial = q.dims == 1;
+        // utils.jl:561-573 check_momentum_dims
+        if (q.pdim != q.dims && !(q.dims == 2 && q.pdim == 3 && !radial))
+            return fail(c, LIM_ERR_ARG,
+                        "momentum_dimensions=%lld with dimensions=%lld is not supported: only (dimensions=2, "
+                        "momentum_dimensions=3) differs from the coupled default.", (long long)q.pdim, (long long)q.dims);
+        if (q.bjorken_redshift) {
+            if (!(q.dims == 2 && q.pdim == 3))
+                return fail(c, LIM_ERR_ARG, "bjorken_redshift requires dimensions=2 and momentum_dimensions=3 (p_z is row 3).");
+            if (!(q.t0 > 0))
+                return fail(c, LIM_ERR_ARG, "bjorken_redshift needs initial_time > 0 (Milne tau; dp_z/dtau = -p_z/tau).");
+        }
+    }
+    if (q.collision < LIM_COLL_LANGEVIN || q.collision > LIM_COLL_FLUID)
+        return fail(c, LIM_ERR_ARG, "collision_mode=%lld is not supported (only :langevin, :rta, :langevin_rta, :fluid).", (long long)q.collision);
+    if (q.integrator_mode != 0 && q.integrator_mode != 1)
+        return fail(c, LIM_ERR_ARG, "integrator_mode must be 0 or 1");
+    if (q.precision != LIM_FP64 && q.precision != LIM_FP32) return fail(c, LIM_ERR_ARG, "precision must be LIM_FP64 or LIM_FP32");
+    if (q.block_size < 0 || q.block_size > 1024 || (q.block_size % 32) != 0)
+        return fail(c, LIM_ERR_ARG, "block_size must be a multiple of 32 in [32, 1024] (or 0)");
+    if (c->have_state && (q.dims != c->dims || q.pdim != c->pdim))
+        return fail(c, LIM_ERR_STATE, "dims/pdim differ from the uploaded state; upload the state again");
+    const bool fo_changed = c->have_state && q.freezeout_capture && !c->P.freezeout_capture;
+    c->P = q;
+    c->have_params = true;
+    if (fo_changed) c->have_state = false;   // latch buffers are allocated at upload
+    return LIM_OK;
+}
+
+int lim_set_medium_rt(lim_ctx* c, const double* xgrid, int64_t nr, const double* tgrid, int64_t nt,
+                      const double* T, const double* V, const double* V2)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!xgrid || !tgrid || !T || !V) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: NULL grid or field");
+    if (nr < 2 || nt < 2) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: need at least 2 nodes per axis (got %lld x %lld)", (long long)nr, (long long)nt);
+    if (!all_finite(xgrid, nr) || !all_finite(tgrid, nt)) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: non-finite grid node");
+    if (!ascending(xgrid, nr) || !ascending(tgrid, nt)) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: grids must be strictly ascending");
+    size_t nn = (size_t)(nr * nt);
+    c->xg.assign(xgrid, xgrid + nr);
+    c->tg.assign(tgrid, tgrid + nt);
+    c->T.assign(T, T + nn);
+    c->V.assign(V, V + nn);
+    if (V2) c->V2.assign(V2, V2 + nn); else c->V2.clear();
+    c->med_kind = MED_RT;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_set_medium_bjorken(lim_ctx* c, double T0, double tau0, double power, double r_max)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!(T0 >= 0) || !(tau0 > 0) || !std::isfinite(power) || !std::isfinite(r_max))
+        return fail(c, LIM_ERR_ARG, "lim_set_medium_bjorken: need T0 >= 0, tau0 > 0, finite power and r_max");
+    c->bj_T0 = T0; c->bj_tau0 = tau0; c->bj_power = power; c->bj_rmax = r_max;
+    c->med_kind = MED_BJORKEN;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_set_medium_grid(lim_ctx* c, int64_t nx, int64_t ny, int64_t nt, double x0, double dx, double y0, double dy,
+                        double tau0, double dtau, const float* T, const float* ux, const float* uy)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!T || !ux || !uy) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: NULL field");
+    if (nx < 2 || ny < 2 || nt < 2) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: need at least 2 nodes per axis");
+    if (!(dx > 0) || !(dy > 0) || !(dtau > 0)) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: spacings must be positive");
+    if (!std::isfinite(x0) || !std::isfinite(y0) || !std::isfinite(tau0)) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: non-finite origin");
+    if ((double)nx * ny * nt > 4.0e9) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: grid too large");
+    size_t nn = (size_t)(nx * ny * nt);
+    c->gT.assign(T, T + nn); c->gux.assign(ux, ux + nn); c->guy.assign(uy, uy + nn);
+    c->gnx = nx; c->gny = ny; c->gnt = nt;
+    c->gx0 = x0; c->gdx = dx; c->gy0 = y0; c->gdy = dy; c->gt0 = tau0; c->gdt = dtau;
+    c->med_kind = MED_GRID;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_set_spline(lim_ctx* c, int which, double Tmin, double invdT, const double* vals, int64_t n)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (which != LIM_SPLINE_DRAG && which != LIM_SPLINE_RTA) return fail(c, LIM_ERR_ARG, "lim_set_spline: unknown spline %d", which);
+    if (!vals || n < 1) return fail(c, LIM_ERR_ARG, "lim_set_spline: empty spline");
+    if (!std::isfinite(Tmin) || !std::isfinite(invdT)) return fail(c, LIM_ERR_ARG, "lim_set_spline: non-finite Tmin/invdT");
+    c->spl[which].assign(vals, vals + n);
+    c->spl_Tmin[which] = Tmin;
+    c->spl_invdT[which] = invdT;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_set_invcdf(lim_ctx* c, const double* vals, int64_t nU, int64_t nT, double Tmin, double invdT)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!vals || nU < 2 || nT < 2) return fail(c, LIM_ERR_ARG, "lim_set_invcdf: need nU >= 2 and nT >= 2");
+    if (!std::isfinite(Tmin) || !std::isfinite(invdT)) return fail(c, LIM_ERR_ARG, "lim_set_invcdf: non-finite Tmin/invdT");
+    c->icdf.assign(vals, vals + nU * nT);
+    c->nU = nU; c->nT = nT; c->ic_Tmin = Tmin; c->ic_invdT = invdT;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_upload_state(lim_ctx* c, const double* x, int64_t dims, const double* p, int64_t pdim, int64_t n)
+{
+    if (!c) return LIM_ERR_ARG;
+    int rc = state_rows_ok(c);
+    if (rc) return rc;
+    if (n < 0) return fail(c, LIM_ERR_ARG, "lim_upload_state: negative particle count");
+    if (n > (int64_t)UINT32_MAX) return fail(c, LIM_ERR_ARG, "lim_upload_state: at most 2^32-1 particles per context");
+    if (dims != c->P.dims || pdim != c->P.pdim)
+        return fail(c, LIM_ERR_ARG, "momentum rows %lld / position rows %lld differ from the parameters (%lld, %lld)",
+                    (long long)pdim, (long long)dims, (long long)c->P.pdim, (long long)c->P.dims);
+    if (n > 0 && (!x || !p)) return fail(c, LIM_ERR_ARG, "lim_upload_state: NULL state");
+    cudaSetDevice(c->device);
+    c->dims = (int)dims; c->pdim = (int)pdim;
+    c->have_state = false;
+    return c->P.precision == LIM_FP32 ? upload_state_impl<float>(c, x, p, n) : upload_state_impl<double>(c, x, p, n);
+}
+
+int lim_download_state(lim_ctx* c, double* x, double* p)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "no particle state uploaded");
+    cudaSetDevice(c->device);
+    return c->state_prec == LIM_FP32 ? download_state_impl<float>(c, x, p) : download_state_impl<double>(c, x, p);
+}
+
+int lim_initial_lab_boost(lim_ctx* c)
+{
+    if (!c) return LIM_ERR_ARG;
+    int rc = check_ready(c);
+    if (rc) return rc;
+    if (c->P.coords == LIM_COORDS_MILNE) return LIM_OK;   // the Milne CPU driver has no step-0 boost
+    cudaSetDevice(c->device);
+    if (c->state_prec == LIM_FP32) {
+        KParams<float> kp;
+        if ((rc = build_kparams<float>(c, kp))) return rc;
+        LIM_CUDA(c, launch_lab_boost<float>(kp, block_of(c), c->stream));
+    } else {
+        KParams<double> kp;
+        if ((rc = build_kparams<double>(c, kp))) return rc;
+        LIM_CUDA(c, launch_lab_boost<double>(kp, block_of(c), c->stream));
+    }
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+int lim_run(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
+            double* hist_x, double* hist_p)
+{
+    if (!c) return LIM_ERR_ARG;
+    int rc = check_ready(c);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(c, LIM_ERR_ARG, "lim_run: negative step count");
+    if (first_step < 0 || first_step + nsteps > (int64_t)UINT32_MAX) return fail(c, LIM_ERR_ARG, "lim_run: steps must lie in [0, 2^32)");
+    if (save_every < 0) return fail(c, LIM_ERR_ARG, "lim_run: negative save_every");
+    cudaSetDevice(c->device);
+    return c->state_prec == LIM_FP32 ? run_impl<float>(c, first_step, nsteps, save_every, first_slot, hist_x, hist_p)
+                                     : run_impl<double>(c, first_step, nsteps, save_every, first_slot, hist_x, hist_p);
+}
+
+int lim_status(lim_ctx* c, int64_t* first_bad_step)
+{
+    if (!c || !first_bad_step) return LIM_ERR_ARG;
+    *first_bad_step = -1;
+    if (!c->d_status.p) return LIM_OK;
+    unsigned long long bad = ULLONG_MAX;
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    LIM_CUDA(c, cudaMemcpy(&bad, c->d_status.p, sizeof bad, cudaMemcpyDeviceToHost));
+    if (bad != ULLONG_MAX) *first_bad_step = (int64_t)bad;
+    return LIM_OK;
+}
+
+int lim_download_freezeout(lim_ctx* c, double* fo_pos, double* fo_mom, double* fo_tau, double* fo_flag)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "no particle state uploaded");
+    cudaSetDevice(c->device);
+    return c->state_prec == LIM_FP32 ? download_fo_impl<float>(c, fo_pos, fo_mom, fo_tau, fo_flag)
+                                     : download_fo_impl<double>(c, fo_pos, fo_mom, fo_tau, fo_flag);
+}
+
+int lim_observables(lim_ctx* c, int from_freezeout, double* out)
+{
+    if (!c || !out) return LIM_ERR_ARG;
+    int rc = check_ready(c);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    return c->state_prec == LIM_FP32 ? observables_impl<float>(c, from_freezeout, out)
+                                     : observables_impl<double>(c, from_freezeout, out);
+}
+
+int lim_record_noise(lim_ctx* c, int64_t first_step, int64_t nsteps)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (nsteps <= 0) { dev_free(c->d_rec); c->rec_steps = 0; return LIM_OK; }
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "upload the state before enabling noise recording");
+    const double bytes = (double)nsteps * kNoiseSlots * (double)c->n * sizeof(double);
+    if (bytes > 8.0e9) return fail(c, LIM_ERR_ARG, "lim_record_noise: buffer of %.3g bytes is too large", bytes);
+    cudaSetDevice(c->device);
+    int rc = dev_alloc(c, c->d_rec, (size_t)bytes);
+    if (rc) return rc;
+    LIM_CUDA(c, cudaMemsetAsync(c->d_rec.p, 0, (size_t)bytes, c->stream));
+    c->rec_first = first_step;
+    c->rec_steps = nsteps;
+    return LIM_OK;
+}
+
+int lim_download_noise(lim_ctx* c, double* out)
+{
+    if (!c || !out) return LIM_ERR_ARG;
+    if (!c->d_rec.p) return fail(c, LIM_ERR_STATE, "noise recording is off");
+    const size_t bytes = (size_t)c->rec_steps * kNoiseSlots * (size_t)c->n * sizeof(double);
+    LIM_CUDA(c, cudaMemcpyAsync(out, c->d_rec.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+int lim_philox_device(lim_ctx* c, const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    if (!c || !ctr || !key || !out) return LIM_ERR_ARG;
+    cudaSetDevice(c->device);
+    int rc = dev_alloc(c, c->d_probe, 16 * sizeof(uint32_t));
+    if (rc) return rc;
+    uint32_t ck[6] = { ctr[0], ctr[1], ctr[2], ctr[3], key[0], key[1] };
+    LIM_CUDA(c, cudaMemcpyAsync(c->d_probe.p, ck, sizeof ck, cudaMemcpyHostToDevice, c->stream));
+    LIM_CUDA(c, launch_philox_probe((const uint32_t*)c->d_probe.p, (uint32_t*)c->d_probe.p + 8, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync(out, (uint32_t*)c->d_probe.p + 8, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+int lim_last_run_stats(lim_ctx* c, double* kernel_ms, int64_t* launches)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (kernel_ms) *kernel_ms = c->last_ms;
+    if (launches) *launches = c->last_launches;
+    return LIM_OK;
+}
+
+}  // extern "C"

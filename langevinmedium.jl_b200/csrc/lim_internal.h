@@ -1,0 +1,32 @@
+// lim_internal.h — launchers shared between the kernel and C-ABI translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "lim_common.cuh"
+
+namespace lim {
+
+constexpr int kObsNum = 12;   // LIM_OBS_NUM
+
+// Fused step kernels over steps [s0, s1).  coords: 0 Cartesian, 1 Milne.
+template <typename R>
+cudaError_t launch_steps(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st);
+
+// Step-0 lab boost (simulate_cpu.jl:160-163).
+template <typename R>
+cudaError_t launch_lab_boost(const KParams<R>& kp, int block, cudaStream_t st);
+
+// Host layout (rows, n) column-major doubles <-> device structure of arrays.
+template <typename R>
+cudaError_t launch_aos_to_soa(const double* src, int rows, int64_t n, R* const* dst, float* const* lo, cudaStream_t st);
+template <typename R>
+cudaError_t launch_soa_to_aos(R* const* src, float* const* lo, int rows, int64_t n, double* dst, cudaStream_t st);
+
+// Observables: block partial sums (FP64) and their fixed-order total.
+template <typename R>
+cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, double width,
+                               double* partials, int64_t nblocks_max, double* out, cudaStream_t st);
+
+cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
+
+}  // namespace lim

@@ -1,0 +1,363 @@
+// lim_kernels.cu — the fused step kernels and their helpers.
+//
+// One thread owns one particle for a whole chunk of steps: the state is loaded
+// once (coalesced structure-of-arrays loads), evolved in registers through every
+// step of the chunk, and stored once.  This replaces the 5-7 launches per step of
+// the reference GPU driver (simulate_gpu.jl:283-392), each of which re-streamed
+// the state and its scratch arrays through HBM.
+#include <climits>
+#include "lim_internal.h"
+#include "lim_step.cuh"
+
+namespace lim {
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&x)[3], float (&xl)[3], R (&p)[3])
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { x[d] = R(0); xl[d] = 0.f; p[d] = R(0); }
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) {
+        x[d] = kp.x[d][i];
+        if (sizeof(R) == 4) xl[d] = kp.xlo[d][i];
+    }
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) p[d] = kp.p[d][i];
+}
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, const R (&x)[3], const float (&xl)[3], const R (&p)[3])
+{
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) {
+        kp.x[d][i] = x[d];
+        if (sizeof(R) == 4) kp.xlo[d][i] = xl[d];
+    }
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
+}
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ bool state_finite(const R (&x)[3], const R (&p)[3])
+{
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) ok &= (bool)isfinite(x[d]);
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) ok &= (bool)isfinite(p[d]);
+    return ok;
+}
+
+template <typename R, int MED, int DIMS, int PDIM>
+__global__ void __launch_bounds__(256)
+k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kp.n) return;
+    R x[3], p[3];
+    float xl[3];
+    load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
+    R flag = R(0), ltau = R(0), lT = R(0);
+    R lpos[3] = { R(0), R(0), R(0) }, lmom[3] = { R(0), R(0), R(0) };
+    if (kp.fo_capture) {
+        flag = kp.fo_flag[i]; ltau = kp.l_tau[i]; lT = kp.l_T[i];
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
+    }
+    const uint32_t pid = (uint32_t)(kp.pid_offset + i);
+    for (int64_t s = s0; s < s1; ++s) {
+        if (kp.stop_fo && flag != R(0)) break;
+        const StepU<R> su = step_uniforms<R, MED>(kp, s);
+        cart_step<R, MED, DIMS, PDIM>(kp, su, i, s, pid, x, xl, p);
+        if (kp.fo_capture) freezeout_latch<R, MED, DIMS, PDIM>(kp, su, i, x, p, flag, lpos, lmom, ltau, lT);
+        if (!state_finite<R, DIMS, PDIM>(x, p)) {
+            atomicMin(kp.first_bad, (unsigned long long)s);
+            break;
+        }
+    }
+    store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
+    if (kp.fo_capture) {
+        kp.l_tau[i] = ltau; kp.l_T[i] = lT;
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos[d];
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom[d];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_milne(const KParams<R> kp, int64_t s0, int64_t s1)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kp.n) return;
+    R x[3], p[3];
+    float xl[3];
+    load_state<R, 2, 2>(kp, i, x, xl, p);
+    const uint32_t pid = (uint32_t)(kp.pid_offset + i);
+    for (int64_t s = s0; s < s1; ++s) {
+        const StepMilne<R> su = milne_uniforms<R>(kp, s);
+        milne_step<R>(kp, su, i, s, pid, x, xl, p);
+        if (!state_finite<R, 2, 2>(x, p)) {
+            atomicMin(kp.first_bad, (unsigned long long)s);
+            break;
+        }
+    }
+    store_state<R, 2, 2>(kp, i, x, xl, p);
+}
+
+template <typename R, int MED, int DIMS, int PDIM>
+__global__ void __launch_bounds__(256)
+k_lab_boost(const KParams<R> kp)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kp.n) return;
+    R x[3], p[3];
+    float xl[3];
+    load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
+    const StepU<R> su = step_uniforms<R, MED>(kp, 0);
+    Local<R> L = local_medium<R, MED, DIMS>(kp, su, x);
+    boost<R, DIMS, PDIM>(kp, L, p, true);
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+static inline unsigned grid_of(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+template <typename R, int MED>
+static cudaError_t launch_cart_med(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
+{
+    const unsigned g = grid_of(kp.n, block);
+    const int dp = kp.dims * 10 + kp.pdim;
+    if (MED == MED_GRID) {
+        if (dp == 22) k_cart<R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1);
+        else if (dp == 23) k_cart<R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1);
+        else return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
+    switch (dp) {
+    case 11: k_cart<R, MED, 1, 1><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 22: k_cart<R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 23: k_cart<R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 33: k_cart<R, MED, 3, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_steps(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st)
+{
+    if (kp.n == 0 || s1 <= s0) return cudaSuccess;
+    if (coords == 1) {
+        k_milne<R><<<grid_of(kp.n, block), block, 0, st>>>(kp, s0, s1);
+        return cudaGetLastError();
+    }
+    switch (kp.med.kind) {
+    case MED_RT: return launch_cart_med<R, MED_RT>(kp, s0, s1, block, st);
+    case MED_BJORKEN: return launch_cart_med<R, MED_BJORKEN>(kp, s0, s1, block, st);
+    case MED_GRID: return launch_cart_med<R, MED_GRID>(kp, s0, s1, block, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename R, int MED>
+static cudaError_t launch_boost_med(const KParams<R>& kp, int block, cudaStream_t st)
+{
+    const unsigned g = grid_of(kp.n, block);
+    const int dp = kp.dims * 10 + kp.pdim;
+    if (MED == MED_GRID) {
+        if (dp == 22) k_lab_boost<R, MED, 2, 2><<<g, block, 0, st>>>(kp);
+        else if (dp == 23) k_lab_boost<R, MED, 2, 3><<<g, block, 0, st>>>(kp);
+        else return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
+    switch (dp) {
+    case 11: k_lab_boost<R, MED, 1, 1><<<g, block, 0, st>>>(kp); break;
+    case 22: k_lab_boost<R, MED, 2, 2><<<g, block, 0, st>>>(kp); break;
+    case 23: k_lab_boost<R, MED, 2, 3><<<g, block, 0, st>>>(kp); break;
+    case 33: k_lab_boost<R, MED, 3, 3><<<g, block, 0, st>>>(kp); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_lab_boost(const KParams<R>& kp, int block, cudaStream_t st)
+{
+    if (kp.n == 0) return cudaSuccess;
+    switch (kp.med.kind) {
+    case MED_RT: return launch_boost_med<R, MED_RT>(kp, block, st);
+    case MED_BJORKEN: return launch_boost_med<R, MED_BJORKEN>(kp, block, st);
+    case MED_GRID: return launch_boost_med<R, MED_GRID>(kp, block, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion
+// ---------------------------------------------------------------------------
+struct RowPtrs3 { void* p[3]; float* lo[3]; };
+
+template <typename R>
+__global__ void k_aos_to_soa(const double* __restrict__ src, int rows, int64_t n, RowPtrs3 dst)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int d = 0; d < rows; ++d) {
+        double v = src[i * rows + d];
+        R h = (R)v;
+        ((R*)dst.p[d])[i] = h;
+        if (dst.lo[d]) dst.lo[d][i] = (float)(v - (double)h);
+    }
+}
+
+template <typename R>
+__global__ void k_soa_to_aos(RowPtrs3 src, int rows, int64_t n, double* __restrict__ dst)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int d = 0; d < rows; ++d) {
+        double v = (double)((const R*)src.p[d])[i];
+        if (src.lo[d]) v += (double)src.lo[d][i];
+        dst[i * rows + d] = v;
+    }
+}
+
+template <typename R>
+cudaError_t launch_aos_to_soa(const double* src, int rows, int64_t n, R* const* dst, float* const* lo, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    RowPtrs3 rp{};
+    for (int d = 0; d < 3; ++d) { rp.p[d] = d < rows ? (void*)dst[d] : nullptr; rp.lo[d] = (lo && d < rows) ? lo[d] : nullptr; }
+    k_aos_to_soa<R><<<grid_of(n, 256), 256, 0, st>>>(src, rows, n, rp);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_soa_to_aos(R* const* src, float* const* lo, int rows, int64_t n, double* dst, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    RowPtrs3 rp{};
+    for (int d = 0; d < 3; ++d) { rp.p[d] = d < rows ? (void*)src[d] : nullptr; rp.lo[d] = (lo && d < rows) ? lo[d] : nullptr; }
+    k_soa_to_aos<R><<<grid_of(n, 256), 256, 0, st>>>(rp, rows, n, dst);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// observables: FP64 block partials, then a fixed-order sum (deterministic)
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256)
+k_obs_partials(const KParams<R> kp, int from_fo, double cut, double width, double* __restrict__ partials)
+{
+    __shared__ double sh[8][kObsNum];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v[kObsNum];
+#pragma unroll
+    for (int k = 0; k < kObsNum; ++k) v[k] = 0.0;
+    if (i < kp.n) {
+        bool use = true;
+        double p[3] = { 0, 0, 0 }, x[3] = { 0, 0, 0 };
+        if (from_fo) {
+            use = kp.fo_flag[i] != R(0);
+            for (int d = 0; d < kp.pdim; ++d) p[d] = (double)kp.fo_mom[d][i];
+            for (int d = 0; d < kp.dims; ++d) x[d] = (double)kp.fo_pos[d][i];
+        } else {
+            for (int d = 0; d < kp.pdim; ++d) p[d] = (double)kp.p[d][i];
+            for (int d = 0; d < kp.dims; ++d) {
+                x[d] = (double)kp.x[d][i];
+                if (sizeof(R) == 4) x[d] += (double)kp.xlo[d][i];
+            }
+        }
+        if (use) {
+            const double m = (double)kp.m;
+            double px = p[0], py = kp.pdim >= 2 ? p[1] : 0.0;
+            double pt2 = px * px + py * py, pt = sqrt(pt2);
+            double p2 = 0.0;
+            for (int d = 0; d < kp.pdim; ++d) p2 += p[d] * p[d];
+            double E = sqrt(m * m + p2), w = m / E;
+            v[0] = 1.0;
+            v[1] = pt;
+            v[2] = pt2 > 0.0 ? (px * px - py * py) / pt2 : 0.0;
+            v[3] = pt > cut ? 1.0 : 0.0;
+            v[4] = 1.0 / (1.0 + exp(-(pt - cut) / width));
+            v[5] = p2;
+            v[6] = E;
+            v[7] = w * p2;
+            v[8] = px;
+            v[9] = w * px;
+            v[10] = kp.pdim == 3 ? p[2] * p[2] : 0.0;
+            double x2 = 0.0;
+            for (int d = 0; d < kp.dims; ++d) x2 += x[d] * x[d];
+            v[11] = x2;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kObsNum; ++k) {
+        double a = v[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+        if (lane == 0) sh[warp][k] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsNum) {
+        double a = 0.0;
+        const int nw = blockDim.x >> 5;
+        for (int w = 0; w < nw; ++w) a += sh[w][threadIdx.x];
+        partials[(int64_t)blockIdx.x * kObsNum + threadIdx.x] = a;
+    }
+}
+
+__global__ void k_obs_total(const double* __restrict__ partials, int64_t nblocks, double* __restrict__ out)
+{
+    // one thread per observable, fixed summation order
+    const int k = threadIdx.x;
+    if (k >= kObsNum) return;
+    double a = 0.0;
+    for (int64_t b = 0; b < nblocks; ++b) a += partials[b * kObsNum + k];
+    out[k] = a;
+}
+
+template <typename R>
+cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, double width,
+                               double* partials, int64_t nblocks_max, double* out, cudaStream_t st)
+{
+    const int64_t nb = kp.n == 0 ? 1 : (kp.n + 255) / 256;
+    if (nb > nblocks_max) return cudaErrorInvalidValue;
+    k_obs_partials<R><<<(unsigned)nb, 256, 0, st>>>(kp, from_fo, cut, width, partials);
+    k_obs_total<<<1, 32, 0, st>>>(partials, nb, out);
+    return cudaGetLastError();
+}
+
+__global__ void k_philox_probe(const uint32_t* ck, uint32_t* out)
+{
+    uint4 r = philox4x32_10(make_uint4(ck[0], ck[1], ck[2], ck[3]), make_uint2(ck[4], ck[5]));
+    out[0] = r.x; out[1] = r.y; out[2] = r.z; out[3] = r.w;
+}
+
+cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st)
+{
+    k_philox_probe<<<1, 1, 0, st>>>(ctr_key, out);
+    return cudaGetLastError();
+}
+
+// explicit instantiations
+template cudaError_t launch_steps<double>(const KParams<double>&, int, int64_t, int64_t, int, cudaStream_t);
+template cudaError_t launch_steps<float>(const KParams<float>&, int, int64_t, int64_t, int, cudaStream_t);
+template cudaError_t launch_lab_boost<double>(const KParams<double>&, int, cudaStream_t);
+template cudaError_t launch_lab_boost<float>(const KParams<float>&, int, cudaStream_t);
+template cudaError_t launch_aos_to_soa<double>(const double*, int, int64_t, double* const*, float* const*, cudaStream_t);
+template cudaError_t launch_aos_to_soa<float>(const double*, int, int64_t, float* const*, float* const*, cudaStream_t);
+template cudaError_t launch_soa_to_aos<double>(double* const*, float* const*, int, int64_t, double*, cudaStream_t);
+template cudaError_t launch_soa_to_aos<float>(float* const*, float* const*, int, int64_t, double*, cudaStream_t);
+template cudaError_t launch_observables<double>(const KParams<double>&, int, double, double, double*, int64_t, double*, cudaStream_t);
+template cudaError_t launch_observables<float>(const KParams<float>&, int, double, double, double*, int64_t, double*, cudaStream_t);
+
+}  // namespace lim

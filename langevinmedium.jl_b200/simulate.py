@@ -1,0 +1,249 @@
+"""``simulate_ensemble_bulk`` for the B200 engine — the drop-in for the reference's
+CPU and GPU paths.
+
+Mirrors ``Simulate.simulate_ensemble_bulk`` (src/simulate.jl:21-141) and its GPU
+twin (src/simulate_gpu_wrapper.jl:15-108, src/simulate_gpu.jl:26-462): the same
+positional arguments, keyword arguments (``Δt`` included), defaults, error
+messages and return values, dispatched on the backend marker exactly as the
+reference dispatches on ``CPUBackend``/``GPUBackend``.  The time loop runs in the
+CUDA engine; this module only prepares tables and copies state in and out.
+
+Additive keywords (not in the reference): ``seed`` (Philox key), ``precision``
+("fp64" | "fp32"), ``collision_mode=:langevin_rta`` with ``tau_R`` / ``eta_over_s``
+(the combined OU + RTA step), ``device``, ``stream``, ``block_size``.
+"""
+from __future__ import annotations
+
+import math
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+from . import transport as tr
+from .backends import B200Backend, B200_GCBackend
+from .utils import append_thermal_pz, check_momentum_dims, radial_reduction
+
+DEFAULT_SEED = 0x4C494D00
+_local = threading.local()
+
+
+def _engine(device: int, stream) -> capi.Engine:
+    """One engine context per (thread, device, stream), reused across calls."""
+    cache = getattr(_local, "engines", None)
+    if cache is None:
+        cache = _local.engines = {}
+    key = (int(device), int(stream or 0))
+    eng = cache.get(key)
+    if eng is None:
+        eng = cache[key] = capi.Engine(device=device, stream=stream)
+    return eng
+
+
+def _sym(x) -> str:
+    s = str(x)
+    return s[1:] if s.startswith(":") else s
+
+
+@dataclass
+class FreezeOut:
+    """The freeze-out NamedTuple of simulate_gpu.jl:396: (pos, mom, tau, flag)."""
+    pos: np.ndarray
+    mom: np.ndarray
+    tau: np.ndarray
+    flag: np.ndarray
+
+    def __iter__(self):
+        return iter((self.pos, self.mom, self.tau, self.flag))
+
+
+def _time_points(t0: float, tf: float, n: int) -> np.ndarray:
+    return np.linspace(t0, tf, n)
+
+
+def simulate_ensemble_bulk(backend, *args, **kwargs):
+    """Dispatch on the backend marker (simulate.jl:21, :117; simulate_gpu_wrapper.jl:15, :74)."""
+    if isinstance(backend, B200Backend):
+        return _simulate_cartesian(*args, **kwargs)
+    if isinstance(backend, B200_GCBackend):
+        return _simulate_milne(*args, **kwargs)
+    raise TypeError(f"simulate_ensemble_bulk: no method for backend {type(backend).__name__} "
+                    "(use B200Backend() or B200_GCBackend())")
+
+
+def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
+                        TemperatureEvolutionn, VelocityEvolutionn, SpaceTimeGrid, *,
+                        N_particles: int = 10_000, Δt: float = 0.001, initial_time: float = 0.0,
+                        final_time: float = 1.0, save_interval: float = 0.1, m: float = 1.0,
+                        DsT: float = 0.2, DsT_linear: bool = False, DsT_slope: float = 1.765,
+                        DsT_offset: float = -0.159, Tfo: float = 0.156, DsT_quad: bool = False,
+                        DsT_Tref: float = 0.0, dimensions: int = 3, cartesian_spatial_sampling=None,
+                        antithetic_momenta: bool = False, position_diffusion: bool = False,
+                        momentum_langevin: bool = True, reflecting_boundary: bool = False,
+                        collision_mode=":langevin", x_init=None, p_init=None, V2Evolutionn=None,
+                        psi2: float = 0.0, freezeout_capture: bool = False, freezeout_interp: bool = True,
+                        integrator_mode: int = 0, relativistic: bool = True, momentum_dimensions: int = 0,
+                        bjorken_redshift: bool = False,
+                        # additive
+                        seed: int = DEFAULT_SEED, precision: str = "fp64", eta_over_s: float = 0.16,
+                        tau_R_factor: float = 5.0, device: int = 0, stream=None, block_size: int = 0,
+                        stop_after_freezeout: bool = True):
+    mode = _sym(collision_mode)
+    if mode not in ("langevin", "rta", "langevin_rta"):
+        raise ValueError(f"simulate_ensemble_bulk(::B200Backend): collision_mode=:{mode} is not supported "
+                         "(only :langevin, :rta and :langevin_rta).")
+    if integrator_mode not in (0, 1):
+        raise ValueError("integrator_mode must be 0 (pre-point exact OU) or 1 (drift-midpoint)")
+    # --- derived parameters (simulate_gpu.jl:65-75) ---
+    total_time = final_time - initial_time
+    steps = int(math.floor(total_time / Δt))
+    save_every = int(round(save_interval / Δt))
+    if save_every == 0:
+        raise ZeroDivisionError("save_interval/Δt rounds to 0 (DivideError in the reference)")
+    num_saves = steps // save_every
+    if freezeout_capture:
+        num_saves = 1
+        save_every = max(steps, 1)
+    xgrid, tgrid = SpaceTimeGrid
+    xgrid = np.asarray(xgrid, dtype=np.float64)
+    tgrid = np.asarray(tgrid, dtype=np.float64)
+    Tfield = np.asarray(TemperatureEvolutionn, dtype=np.float64)
+    Vfield = np.asarray(VelocityEvolutionn, dtype=np.float64)
+    rng = np.random.default_rng(int(seed) & 0xFFFFFFFFFFFFFFFF)
+    # --- initial state (simulate_cpu.jl:63-94) ---
+    if x_init is None or p_init is None:
+        raise NotImplementedError("the B200 backend takes the initial state from x_init/p_init; "
+                                  "sample it with the reference's samplers (utils.jl) and pass it in")
+    x_matrix = np.array(x_init, dtype=np.float64, ndmin=2)
+    p_matrix = np.array(p_init, dtype=np.float64, ndmin=2)
+    radial_mode = dimensions == 1
+    if radial_mode:
+        if x_matrix.shape[0] >= 2:
+            positions, momenta = radial_reduction(x_matrix[:2], p_matrix[:2], r_grid_Langevin, rng)
+        else:
+            positions, momenta = x_matrix, p_matrix
+    else:
+        positions, momenta = x_matrix.copy(), p_matrix.copy()
+    pdim = dimensions if momentum_dimensions <= 0 else momentum_dimensions
+    check_momentum_dims(dimensions, pdim, radial_mode, bjorken_redshift, initial_time)
+    if momenta.shape[0] < pdim:
+        from .utils import _rt_interp_host
+        momenta = append_thermal_pz(momenta, positions, m,
+                                    lambda r: _rt_interp_host(xgrid, tgrid, Tfield, r, initial_time),
+                                    antithetic=antithetic_momenta and x_init is None, rng=rng)
+    if momenta.shape[0] != pdim:
+        raise ValueError(f"momentum rows {momenta.shape[0]} ≠ momentum_dimensions {pdim}")
+    if positions.shape[0] != dimensions:
+        raise ValueError(f"position rows {positions.shape[0]} ≠ dimensions {dimensions}")
+    N = positions.shape[1]
+    if momenta.shape[1] != N:
+        raise ValueError("x_init and p_init hold different particle counts")
+
+    # --- engine configuration ---
+    if not momentum_langevin or DsT == 0.0:
+        coll = capi.LIM_COLL_FLUID
+    elif mode == "rta":
+        coll = capi.LIM_COLL_RTA
+    elif mode == "langevin_rta":
+        coll = capi.LIM_COLL_LANGEVIN_RTA
+    else:
+        coll = capi.LIM_COLL_LANGEVIN
+    eng = _engine(device, stream)
+    eng.set_params(dt=Δt, t0=initial_time, m=m, DsT=DsT, Tfo=Tfo, psi2=psi2, dims=dimensions, pdim=pdim,
+                   coords=capi.LIM_COORDS_CARTESIAN, collision=coll, relativistic=int(bool(relativistic)),
+                   bjorken_redshift=int(bool(bjorken_redshift)), position_diffusion=int(bool(position_diffusion)),
+                   reflecting_boundary=int(bool(reflecting_boundary)), integrator_mode=integrator_mode,
+                   freezeout_capture=int(bool(freezeout_capture)), freezeout_interp=int(bool(freezeout_interp)),
+                   precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64, seed=seed,
+                   stop_after_freezeout=int(bool(stop_after_freezeout and freezeout_capture)), block_size=block_size)
+    eng.set_medium_rt(xgrid, tgrid, Tfield, Vfield, V2Evolutionn)
+    # --- transport tables (simulate_gpu.jl:90-138) ---
+    if momentum_langevin and DsT > 0.0:
+        Tmin, Tmax = tr.spline_range(Tfield)
+        dkw = dict(Tmin=Tmin, Tmax=Tmax, nT=1024, DsT_linear=DsT_linear, DsT_slope=DsT_slope,
+                   DsT_offset=DsT_offset, Tfo=Tfo, DsT_quad=DsT_quad, DsT_Tref=DsT_Tref)
+        t0_, inv_, vals = tr.build_tau_drag_spline(m, DsT, **dkw)
+        eng.set_spline(capi.LIM_SPLINE_DRAG, t0_, inv_, vals)
+        if mode == "rta":
+            _, _, nvals = tr.build_taun_current_spline(m, DsT, **dkw)
+            eng.set_spline(capi.LIM_SPLINE_RTA, t0_, inv_, nvals)
+        elif mode == "langevin_rta":
+            _, _, rvals = tr.build_tau_R_spline(m, DsT, eta_over_s=eta_over_s, factor=tau_R_factor, **dkw)
+            eng.set_spline(capi.LIM_SPLINE_RTA, t0_, inv_, rvals)
+        if mode in ("rta", "langevin_rta"):
+            inv, nU, nT, Ttmin, Tinv = tr.build_juttner_invcdf(m, pdim, Tmin=Tmin, Tmax=Tmax, nT=256, nU=2048, np_=8192)
+            eng.set_invcdf(inv, nU, nT, Ttmin, Tinv)
+    elif mode in ("rta", "langevin_rta"):
+        eng.set_invcdf(np.zeros(4), 2, 2, 0.0, 1.0)   # reference default table (simulate_gpu.jl:124-128)
+    eng.upload_state(positions, momenta)
+    eng.initial_lab_boost()
+
+    if freezeout_capture:
+        eng.run(1, steps)
+        fo = eng.download_freezeout()
+        return FreezeOut(fo["pos"], fo["mom"], fo["tau"], fo["flag"])
+
+    nslots = num_saves + 1
+    hx = np.empty(nslots * N * dimensions)
+    hp = np.empty(nslots * N * pdim)
+    eng.download_state_flat(hx[: N * dimensions], hp[: N * pdim])
+    eng.run(1, steps, save_every, 0, hx, hp)
+    time_points = _time_points(initial_time, final_time, nslots)
+    mom = [hp[k * N * pdim:(k + 1) * N * pdim].reshape(N, pdim).T for k in range(nslots)]
+    pos = [hx[k * N * dimensions:(k + 1) * N * dimensions].reshape(N, dimensions).T for k in range(nslots)]
+    return time_points, mom, pos
+
+
+def _simulate_milne(T_profile_MIS, ur_profile_MIS, mu_profile_MIS, TemperatureEvolutionn, VelocityEvolutionn,
+                    SpaceTimeGrid, *, N_particles: int = 10_000, Δt: float = 0.001, initial_time: float = 0.0,
+                    final_time: float = 1.0, save_interval: float = 0.1, m: float = 1.0, DsT: float = 0.2,
+                    dimensions: int = 2, x_init=None, p_init=None, seed: int = DEFAULT_SEED,
+                    precision: str = "fp64", device: int = 0, stream=None, block_size: int = 0):
+    """Milne (tau, r) driver (simulate_cpu_general_coords.jl:18-133)."""
+    if dimensions != 2:
+        raise ValueError("Milne coordinates evolve (τ, r): dimensions must be 2")
+    total_time = final_time - initial_time
+    steps = int(math.floor(total_time / Δt))
+    q = save_interval / Δt
+    if q != math.floor(q):
+        raise ValueError(f"InexactError: Int64({q})")          # Int(save_interval/Δt)
+    save_every = int(q)
+    num_saves = steps // save_every
+    xgrid, tgrid = SpaceTimeGrid
+    Tfield = np.asarray(TemperatureEvolutionn, dtype=np.float64)
+    if x_init is None or p_init is None:
+        raise NotImplementedError("the B200 Milne backend takes the initial (τ, r), (p^τ, p^r) from x_init/p_init")
+    positions = np.array(x_init, dtype=np.float64, ndmin=2)
+    momenta = np.array(p_init, dtype=np.float64, ndmin=2)
+    N = positions.shape[1]
+    eng = _engine(device, stream)
+    eng.set_params(dt=Δt, t0=initial_time, m=m, DsT=DsT, dims=2, pdim=2, coords=capi.LIM_COORDS_MILNE,
+                   collision=capi.LIM_COLL_LANGEVIN, precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64,
+                   seed=seed, block_size=block_size)
+    eng.set_medium_rt(np.asarray(xgrid, dtype=np.float64), np.asarray(tgrid, dtype=np.float64), Tfield,
+                      np.asarray(VelocityEvolutionn, dtype=np.float64))
+    if DsT > 0.0:
+        Tmin, Tmax = tr.spline_range(Tfield)
+        t0_, inv_, vals = tr.build_tau_drag_spline(m, DsT, Tmin=Tmin, Tmax=Tmax, nT=1024)
+        eng.set_spline(capi.LIM_SPLINE_DRAG, t0_, inv_, vals)
+    eng.upload_state(positions, momenta)
+    nslots = num_saves + 1
+    hx = np.empty(nslots * N * 2)
+    hp = np.empty(nslots * N * 2)
+    eng.download_state_flat(hx[: N * 2], hp[: N * 2])
+    try:
+        eng.run(1, steps, save_every, 0, hx, hp)
+    except capi.LimError as e:          # the Milne CPU driver has no NaN/Inf check
+        if e.code != capi.LIM_ERR_NONFINITE:
+            raise
+    time_points = _time_points(initial_time, final_time, nslots)
+    momenta_history = []
+    position_history = []
+    for k in range(nslots):
+        P = hp[k * N * 2:(k + 1) * N * 2].reshape(N, 2)
+        X = hx[k * N * 2:(k + 1) * N * 2].reshape(N, 2)
+        # simulate_cpu_general_coords.jl:53-55 and :120-124: |p| over (p^τ, p^r) and the r row
+        momenta_history.append(np.abs(P[:, 1]) if k == 0 else np.sqrt(np.sum(P ** 2, axis=1)))
+        position_history.append(X[:, 1].reshape(1, N).copy())
+    return time_points, momenta_history, position_history

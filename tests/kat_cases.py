@@ -1,0 +1,116 @@
+"""The dynamical known-answer tests of the reference (test/test_momentum_dims3.jl and
+test/test_relativistic_switch.jl), written once over a `box_run` driver so that the
+same assertions run on the CPU restatement (tests/test_oracle_kats.py) and on the
+B200 engine through the public API (tests/test_gpu_physics.py)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from helpers import HBARC_TEST, K2K3, est, juttner_sample, lam1, p2eq
+
+M_, T_ = 1.5, 0.30
+DST_ = 0.11634
+ETA_ = (T_ ** 2 / (M_ * DST_)) / HBARC_TEST
+DS_FM = (DST_ / T_) * HBARC_TEST
+
+
+def case_equilibria(box_run):
+    """(E) test_momentum_dims3.jl:119-143."""
+    N_E, dt_E, tfin_E = 150_000, 2e-3, 4.0
+    rng = np.random.default_rng(11)
+    x0 = np.zeros((2, N_E))
+    p0_3 = 0.9 * rng.standard_normal((3, N_E))
+    p0_2 = p0_3[:2].copy()
+    _, m3, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_E, dt=dt_E, tfinal=tfin_E, save=0.5, x0=x0, p0=p0_3, pdim=3)
+    _, m2, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_E, dt=dt_E, tfinal=tfin_E, save=0.5, x0=x0, p0=p0_2, pdim=2)
+    e3, e2 = est(m3[-1], M_), est(m2[-1], M_)
+    assert m3[-1].shape[0] == 3 and m2[-1].shape[0] == 2
+    assert math.isclose(e3["p2"], p2eq(M_, T_, 3), rel_tol=0.015)
+    assert math.isclose(e2["p2"], p2eq(M_, T_, 2), rel_tol=0.015)
+    assert math.isclose(e3["lam"], K2K3(M_ / T_), rel_tol=0.005)
+    assert math.isclose(e2["lam"], lam1(M_, T_, 2), rel_tol=0.005)
+    assert e2["lam"] / e3["lam"] > 1.06
+    assert math.isclose(np.mean(m3[-1][2] ** 2), np.mean(m3[-1][0] ** 2), rel_tol=0.02)
+    return e3, e2
+
+
+def case_l1_decay(box_run):
+    """(D) test_momentum_dims3.jl:145-171."""
+    v = 0.05
+    g = 1 / math.sqrt(1 - v * v)
+    N_D = 400_000
+    rates, refs = {}, {}
+    for d in (3, 2):
+        P = juttner_sample(np.random.default_rng(100 + d), M_, T_, d, N_D)
+        E = np.sqrt(M_ ** 2 + np.sum(P ** 2, axis=0))
+        P[0] = g * (P[0] + v * E)
+        tt, mm, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_D, dt=1e-3, tfinal=0.30, save=0.05,
+                            x0=np.zeros((2, N_D)), p0=P, pdim=d, seed=5 + d)
+        jx = np.array([est(m, M_)["jx"] for m in mm])
+        tt = np.asarray(tt)
+        r_inst = ETA_ * est(mm[0], M_)["jxw"] / est(mm[0], M_)["jx"]
+        A = np.vstack([np.ones_like(tt), tt]).T
+        c = np.linalg.lstsq(A, np.log(jx), rcond=None)[0]
+        rates[d] = -c[1]
+        refs[d] = (K2K3(M_ / T_) if d == 3 else lam1(M_, T_, d)) * ETA_
+        assert math.isclose(r_inst, refs[d], rel_tol=0.012)
+        assert math.isclose(rates[d], refs[d], rel_tol=0.04)
+    assert rates[2] / rates[3] > 1.05
+    return rates
+
+
+def case_bjorken_redshift(box_run):
+    """(R) test_momentum_dims3.jl:173-188: exact telescoping to 1e-9."""
+    N_R, t0, tf, dt = 20_000, 0.4, 2.0, 1e-3
+    rng = np.random.default_rng(3)
+    P = np.vstack([0.3 * rng.standard_normal((2, N_R)), 0.5 * rng.standard_normal((1, N_R))])
+    tt, mm, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_R, dt=dt, tfinal=tf, save=0.4, x0=4.0 * np.ones((2, N_R)),
+                        p0=P, pdim=3, t0=t0, redshift=True, momentum_langevin=False)
+    ref0 = np.mean(P[2] ** 2)
+    for k, tau in enumerate(tt):
+        assert math.isclose(np.mean(mm[k][2] ** 2), ref0 * (t0 / tau) ** 2, rel_tol=1e-9)
+
+
+def case_msd(box_run):
+    """(M) test_momentum_dims3.jl:190-201: MSD slope = 4 D_s."""
+    N_M, tf = 100_000, 8.0
+    P = juttner_sample(np.random.default_rng(3), M_, T_, 3, N_M)
+    tt, _, xx = box_run(M=M_, T=T_, DsT=DST_, N=N_M, dt=2e-3, tfinal=tf, save=0.5, x0=50.0 * np.ones((2, N_M)),
+                        p0=P, pdim=3, seed=9)
+    msd = np.array([np.mean(np.sum((x - xx[0]) ** 2, axis=0)) for x in xx])
+    tt = np.asarray(tt)
+    sel = tt >= 4.0
+    A = np.vstack([np.ones(sel.sum()), tt[sel]]).T
+    c = np.linalg.lstsq(A, msd[sel], rcond=None)[0]
+    Ds_meas = c[1] / 4
+    assert math.isclose(Ds_meas, DS_FM, rel_tol=0.03)
+    return Ds_meas
+
+
+def case_relativistic_switch(box_run):
+    """test_relativistic_switch.jl:67-94 through the full step (drag, kick and streaming)."""
+    M, T, DsT, N, dt, nsteps = 1.5, 0.3, 0.5, 20_000, 2e-3, 4000
+    rng = np.random.default_rng(20260806)
+    p0 = 0.9 * rng.standard_normal((2, N))
+    x0 = np.zeros((2, N))
+    res = {}
+    for rel in (True, False):
+        _, mm, xx = box_run(M=M, T=T, DsT=DsT, N=N, dt=dt, tfinal=nsteps * dt, save=nsteps * dt, x0=x0, p0=p0,
+                            pdim=2, relativistic=rel, seed=20260806)
+        res[rel] = (mm[-1], xx[-1])
+    pr, xr = res[True]
+    pn, xn = res[False]
+    p2r = np.mean(np.sum(pr ** 2, axis=0))
+    p2n = np.mean(np.sum(pn ** 2, axis=0))
+    juttner_p2 = 2 * T * (M * M + 3 * M * T + 3 * T * T) / (M + T)
+    maxwell_p2 = 2 * M * T
+    assert not math.isclose(p2r, p2n, rel_tol=1e-6)
+    assert math.isclose(p2r, juttner_p2, rel_tol=0.04)
+    assert math.isclose(p2n, maxwell_p2, rel_tol=0.04)
+    assert juttner_p2 / maxwell_p2 > 1.2
+    x2r = np.mean(np.sum(xr ** 2, axis=0))
+    x2n = np.mean(np.sum(xn ** 2, axis=0))
+    assert not math.isclose(x2r, x2n, rel_tol=1e-3)
+    assert x2n > x2r
