@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput of the fused heavy-quark Langevin step on B200.
+
+Workload (one benchmark "step" = one full simulation pass): the Bjorken medium
+T(tau) = 0.40 (0.6/tau)^(1/3) GeV as a reference (r, t) table, tau 0.6 -> 10 fm/c
+with dtau = 0.005 (1880 steps), 1e6 charm quarks per GPU (p_T power law, uniform
+phi and rapidity), Langevin (2 pi T D_s = 4) plus RTA (tau_R = 5 eta/s / T), Bjorken
+redshift, FP32 arithmetic with FP64 momentum accumulation.  Synthetic seeded inputs.
+
+  value : particle-steps/s over all GPUs, inputs resident in HBM (state restored from a
+          device checkpoint before every pass); L2 flushed between passes.
+  e2e   : the same through the C-ABI from pinned host buffers: upload, step-0 boost,
+          run, download of the final state, every pass.
+
+`--impl reference` times the reference's CPU algorithm (the FP64 restatement under
+oracle/, all host threads) on a bounded sample of the same workload.
+Multi-GPU (torchrun): every rank runs its own 1e6 particles (weak scaling, no
+data-path collective); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s on 1 B200 (plain vs batched; fwd+adjoint cost) at ≤1e-5 rel err"
+WORKLOAD = "bjorken_langevin_rta_1e6_charm_fp32"
+
+
+def load_package():
+    import __graft_entry__ as ge
+    return ge.load_package()
+
+
+# ---------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons, power = [], None, set(), []
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------------
+# the reference CPU arm and the CPU baseline (FP64 restatement, all host threads)
+# ---------------------------------------------------------------------------------
+def cpu_sample(pkg, n_particles: int, threads: int = 0, calib_steps: int = 0):
+    """Run the restatement on a bounded sample of the workload; returns (particle-steps/s, info)."""
+    from oracle import oracle as orc
+    W = pkg.workloads
+    wl = W.bjorken(N=n_particles, precision="fp64", rng_seed=2)
+    steps = calib_steps or wl.steps
+    P = orc.make_params(**dict(wl.params, precision=0))
+    md = orc.Medium().rt(wl.medium["xgrid"], wl.medium["tgrid"], wl.medium["T"], wl.medium["V"])
+    for w, (a, b, v) in wl.splines.items():
+        md.spline(w, a, b, v)
+    md.invcdf(*wl.invcdf)
+    x0, p0 = orc.initial_lab_boost(P, md, wl.x, wl.p)
+    t = time.perf_counter()
+    orc.run(P, md, x0, p0, wl.first_step, steps, threads=threads)
+    dt = time.perf_counter() - t
+    return n_particles * steps / dt, dict(particles=n_particles, steps=steps, seconds=dt)
+
+
+def size_cpu_sample(pkg, target_s: float, threads: int) -> int:
+    """Particles for ~target_s seconds of the full 1880-step run on `threads` threads."""
+    from oracle import oracle as orc
+    n0 = 512 * max(1, threads or orc.max_threads())
+    rate, _ = cpu_sample(pkg, n0, threads, calib_steps=60)
+    return max(256, int(rate * target_s / 1880))
+
+
+def run_reference(args, rank: int, world: int):
+    if rank != 0:
+        return
+    pkg = load_package()
+    from oracle import oracle as orc
+    threads = orc.max_threads()
+    n = size_cpu_sample(pkg, 6.0, threads)
+    for _ in range(args.warmup):
+        cpu_sample(pkg, max(256, n // 8), threads)
+    vals = []
+    total_ps, total_s = 0, 0.0
+    for _ in range(args.steps):
+        v, info = cpu_sample(pkg, n, threads)
+        vals.append(v)
+        total_ps += info["particles"] * info["steps"]
+        total_s += info["seconds"]
+    value = total_ps / total_s
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Bjorken workload sample)",
+        "config": {"workload": WORKLOAD, "particles_per_step_sample": n, "steps_per_pass": 1880,
+                   "note": "the reference is Julia (not installed); this arm times its CPU algorithm as the "
+                           "C FP64 restatement under oracle/ on all host threads"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} charm quarks x 1880 steps per timed step"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------
+def work_model(pkg):
+    wm = json.loads((Path(pkg.__file__).parent / "work_model.json").read_text())
+    w = wm["workloads"]["bjorken_langevin_rta_fp32"]
+    tot = {}
+    for item in w["items"].values():
+        for k, c in item.items():
+            tot[k] = tot.get(k, 0.0) + c
+    return tot, sum(tot.values()), w["hbm_bytes_per_particle_per_launch"]
+
+
+def traffic_from_profile():
+    p = ROOT / "profiles" / "k_cart_bjorken_fp32_traffic.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return d.get("bytes_per_launch_full_size")
+        except (ValueError, KeyError):
+            return None
+    return None
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pkg = load_package()
+    W = pkg.workloads
+    capi = pkg.capi
+    n = args.particles
+    stream = torch.cuda.current_stream()
+    wl = W.bjorken(N=n, precision="fp32", rng_seed=2 + rank)
+    wl.params["particle_offset"] = rank * n              # global particle ids: each rank its own noise streams
+    eng = capi.Engine(device=local_rank, stream=stream.cuda_stream)
+    W.configure(eng, wl)
+    eng.initial_lab_boost()
+    eng.state_save()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")   # > 126 MB L2
+
+    def one_pass():
+        eng.state_restore()
+        eng.run(wl.first_step, wl.steps)
+
+    for _ in range(args.warmup):
+        one_pass()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    pass_ms, kern_ms = [], []
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()                                    # between timed iterations, not timed
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one_pass()
+        e1.record(stream)
+        e1.synchronize()
+        pass_ms.append(e0.elapsed_time(e1))
+        k, nl = eng.last_run_stats()
+        kern_ms.append(k)
+        launches += nl
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = float(sum(pass_ms))
+    t = torch.tensor([total_ms, float(sum(kern_ms))], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, total_kern_ms = float(t[0]), float(t[1])
+    ps_per_pass = n * wl.steps
+    value = world * ps_per_pass * args.steps / (total_ms * 1e-3)
+
+    # physics output of the last pass, reduced over ranks (FP64 observable sums)
+    obs = eng.observables()
+    sums = torch.tensor(obs["sums"], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(sums)
+
+    # ---- e2e through the C-ABI with pinned host buffers ----
+    dims, pdim = 2, 3
+    x_host = torch.from_numpy(capi.julia_layout(wl.x, dims).copy()).pin_memory()
+    p_host = torch.from_numpy(capi.julia_layout(wl.p, pdim).copy()).pin_memory()
+    x_out = torch.empty(n * dims, dtype=torch.float64).pin_memory()
+    p_out = torch.empty(n * pdim, dtype=torch.float64).pin_memory()
+    xb, pb, xo, po = (a.numpy() for a in (x_host, p_host, x_out, p_out))
+    e2e_launches = 0
+
+    def e2e_pass():
+        eng.upload_state_flat(xb, pb, n)
+        eng.initial_lab_boost()
+        eng.run(wl.first_step, wl.steps)
+        eng.download_state_flat(xo, po)
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_pass()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_pass()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        e2e_launches += 7          # 2 uploads + boost + table + step + 2 downloads
+    te = torch.tensor([float(sum(e2e_ms))], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * ps_per_pass * args.steps / (float(te[0]) * 1e-3)
+
+    # ---- roofline of the step kernel ----
+    counts, i_alg, hbm_pp = work_model(pkg)
+    fma_rate, _ = eng.probe_fma_rate()                    # measured FP32 issue ceiling (thread-instr/s)
+    kern_s = (total_kern_ms / args.steps) * 1e-3
+    achieved = i_alg * ps_per_pass / kern_s               # algorithmic thread-instructions per second
+    bytes_launch = hbm_pp * n
+    roofline = {
+        "bound": "issue", "unit": "Ginst/s",
+        "achieved": achieved / 1e9, "peak": fma_rate / 1e9, "frac": achieved / fma_rate,
+        "traffic": traffic_from_profile(),
+        "kernel": "k_cart (fused Langevin+RTA step, 1880 steps per launch)",
+        "algorithmic_inst_per_particle_step": i_alg,
+        "inst_mix_per_particle_step": counts,
+        "peak_source": "measured in this run: FP32 FMA issue probe (lim_probe_fma_rate), thread-instr/s",
+        "kernel_ms_per_launch": kern_s * 1e3,
+        "hbm": {"algorithmic_bytes_per_launch": bytes_launch, "achieved_gbs": bytes_launch / kern_s / 1e9,
+                "peak_gbs": 6544.3, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+    }
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        threads = orc.max_threads()
+        ncpu = size_cpu_sample(pkg, 12.0, threads)
+        rate, info = cpu_sample(pkg, ncpu, threads)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{ncpu} charm quarks x 1880 steps of the same workload, FP64 restatement (oracle/), "
+                         f"{info['seconds']:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Bjorken workload)",
+            "config": {"workload": WORKLOAD, "particles_per_gpu": n, "steps_per_pass": wl.steps,
+                       "particle_steps_per_pass_per_gpu": ps_per_pass, "medium": "reference (r,t) table 41x1883",
+                       "collision": "langevin+rta", "precision": "fp32 arithmetic, fp64 momentum accumulation",
+                       "l2": "flushed between timed passes (256 MB write)", "parallelism": f"dp{world} (particles)"},
+            "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": int(xb.nbytes + pb.nbytes), "d2h_bytes_per_step": int(xo.nbytes + po.nbytes)},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "observables": {k: float(v) for k, v in zip(capi.OBS_NAMES, (sums.cpu().numpy() /
+                                                                       max(float(sums[0]), 1.0)))},
+        }
+        line["observables"]["count"] = float(sums[0])
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--particles", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

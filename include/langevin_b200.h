@@ -167,6 +167,13 @@ int lim_upload_state(lim_ctx* ctx, const double* x, int64_t dims,
                      const double* p, int64_t pdim, int64_t n);
 int lim_download_state(lim_ctx* ctx, double* x, double* p);
 
+/* Device-side checkpoint of the particle state (and freeze-out latch): save
+ * copies it into a device buffer owned by the context, restore copies it back.
+ * With the counter-based noise, (state, step) fully determines the continuation,
+ * so a restore followed by lim_run(step, ...) reproduces the original run. */
+int lim_state_save(lim_ctx* ctx);
+int lim_state_restore(lim_ctx* ctx);
+
 /* The step-0 lab boost applied before the loop (simulate_cpu.jl:160-163). */
 int lim_initial_lab_boost(lim_ctx* ctx);
 

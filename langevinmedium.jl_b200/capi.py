@@ -15,6 +15,7 @@ import numpy as np
 PKG_DIR = Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "liblangevin_b200.so"
 HEADER = PKG_DIR.parent / "include" / "langevin_b200.h"
+DIAG_HEADER = PKG_DIR.parent / "include" / "langevin_b200_diag.h"
 
 LIM_OK, LIM_ERR_ARG, LIM_ERR_CUDA, LIM_ERR_STATE, LIM_ERR_NONFINITE, LIM_ERR_TIMEOUT, LIM_ERR_UNSUPPORTED, LIM_ERR_NOMEM = \
     0, -1, -2, -3, -4, -5, -6, -7
@@ -69,6 +70,8 @@ _SIGS = {
     "lim_upload_state": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, C.c_int64], C.c_int),
     "lim_download_state": ([C.c_void_p, _DP, _DP], C.c_int),
     "lim_initial_lab_boost": ([C.c_void_p], C.c_int),
+    "lim_state_save": ([C.c_void_p], C.c_int),
+    "lim_state_restore": ([C.c_void_p], C.c_int),
     "lim_run": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
     "lim_status": ([C.c_void_p, _I64P], C.c_int),
     "lim_download_freezeout": ([C.c_void_p, _DP, _DP, _DP, _DP], C.c_int),
@@ -77,6 +80,7 @@ _SIGS = {
     "lim_download_noise": ([C.c_void_p, _DP], C.c_int),
     "lim_philox_device": ([C.c_void_p, _U32P, _U32P, _U32P], C.c_int),
     "lim_last_run_stats": ([C.c_void_p, _DP, _I64P], C.c_int),
+    "lim_probe_fma_rate": ([C.c_void_p, _DP, _DP], C.c_int),
 }
 
 
@@ -241,6 +245,12 @@ class Engine:
     def download_state_flat(self, xbuf: np.ndarray | None, pbuf: np.ndarray | None):
         self._check(self.lib.lim_download_state(self.ctx, _dptr(xbuf), _dptr(pbuf)))
 
+    def state_save(self):
+        self._check(self.lib.lim_state_save(self.ctx))
+
+    def state_restore(self):
+        self._check(self.lib.lim_state_restore(self.ctx))
+
     def initial_lab_boost(self):
         self._check(self.lib.lim_initial_lab_boost(self.ctx))
 
@@ -292,6 +302,13 @@ class Engine:
         nl = C.c_int64(0)
         self._check(self.lib.lim_last_run_stats(self.ctx, C.byref(ms), C.byref(nl)))
         return ms.value, int(nl.value)
+
+    def probe_fma_rate(self):
+        """(thread FMA instructions per second, probe ms) of the FP32 FMA issue probe."""
+        r = C.c_double(0.0)
+        ms = C.c_double(0.0)
+        self._check(self.lib.lim_probe_fma_rate(self.ctx, C.byref(r), C.byref(ms)))
+        return r.value, ms.value
 
     def device_bytes(self) -> int:
         v = C.c_int64(0)

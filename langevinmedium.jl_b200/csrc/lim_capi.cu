@@ -13,6 +13,7 @@
 #include <string>
 #include <vector>
 #include "../../include/langevin_b200.h"
+#include "../../include/langevin_b200_diag.h"
 #include "lim_internal.h"
 
 using namespace lim;
@@ -54,7 +55,7 @@ struct lim_ctx {
     // device copy of the medium for `dev_prec`
     int dev_prec = -1;
     bool dev_dirty = true;
-    DevBuf d_xg, d_tg, d_tgd, d_TV, d_V2, d_G, d_spl[2], d_icdf;
+    DevBuf d_xg, d_tg, d_tgd, d_xgd, d_TV, d_V2, d_G, d_spl[2], d_icdf;
 
     // particle state (structure of arrays, precision `state_prec`)
     int64_t n = 0;
@@ -62,9 +63,9 @@ struct lim_ctx {
     bool have_state = false;
     DevBuf d_x[3], d_xlo[3], d_p[3];
     DevBuf d_fo_pos[3], d_fo_mom[3], d_fo_tau, d_fo_flag, d_l_pos[3], d_l_mom[3], d_l_tau, d_l_T;
-    DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe;
-    DevBuf d_rec;
-    int64_t rec_first = 0, rec_steps = 0;
+    DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe, d_steps;
+    DevBuf d_rec, d_ckpt;
+    int64_t rec_first = 0, rec_steps = 0, ckpt_n = -1;
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -167,6 +168,7 @@ int ensure_device_medium(lim_ctx* c)
         if ((rc = upload(c, c->d_xg, xr.data(), nr))) return rc;
         if ((rc = upload(c, c->d_tg, tr.data(), nt))) return rc;
         if ((rc = upload(c, c->d_tgd, c->tg.data(), nt))) return rc;
+        if ((rc = upload(c, c->d_xgd, c->xg.data(), nr))) return rc;
         if ((rc = upload(c, c->d_TV, tv.data(), tv.size()))) return rc;
         if (!c->V2.empty()) {
             std::vector<R> v2(c->V2.size());
@@ -216,6 +218,20 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
     kp.drag_Tmin = (R)c->spl_Tmin[0]; kp.drag_invdT = (R)c->spl_invdT[0];
     kp.rta = (const R*)c->d_spl[1].p; kp.n_rta = (int)c->spl[1].size();
     kp.rta_Tmin = (R)c->spl_Tmin[1]; kp.rta_invdT = (R)c->spl_invdT[1];
+    if (sizeof(R) == 4) {
+        // A spline whose whole T range is narrower than FP32 resolves (the drivers build
+        // [Tmin, Tmin + eps] for a uniform field, simulate_cpu.jl:191-192) is a constant
+        // to FP32 accuracy; evaluating it as one avoids extrapolating over ~1e11 cells.
+        for (int w = 0; w < 2; ++w) {
+            const size_t n = c->spl[w].size();
+            if (n >= 2) {
+                const double width = (double)(n - 1) / c->spl_invdT[w];
+                if (std::fabs(width) <= 1e-6 * std::fabs(c->spl_Tmin[w])) {
+                    if (w == 0) kp.n_drag = 1; else kp.n_rta = 1;
+                }
+            }
+        }
+    }
     kp.icdf = (const R*)c->d_icdf.p; kp.nU = (int)c->nU; kp.nT = (int)c->nT;
     kp.ic_Tmin = (R)c->ic_Tmin; kp.ic_invdT = (R)c->ic_invdT;
     MediumDev<R>& md = kp.med;
@@ -223,6 +239,7 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
     md.T_scale = (R)c->T_scale;
     if (c->med_kind == MED_RT) {
         md.xg = (const R*)c->d_xg.p; md.tg = (const R*)c->d_tg.p; md.tgd = (const double*)c->d_tgd.p;
+        md.xgd = (const double*)c->d_xgd.p;
         md.nr = (int)c->xg.size(); md.nt = (int)c->tg.size();
         double x0, xi, t0g, ti;
         md.x_uniform = near_uniform(c->xg, x0, xi); md.xg0 = (R)x0; md.xinvd = (R)xi;
@@ -246,12 +263,12 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
         md.r_max = (R)r; md.r_axis_eps = (R)1e-6;
     }
     for (int d = 0; d < 3; ++d) {
-        kp.x[d] = (R*)c->d_x[d].p; kp.xlo[d] = (float*)c->d_xlo[d].p; kp.p[d] = (R*)c->d_p[d].p;
-        kp.fo_pos[d] = (R*)c->d_fo_pos[d].p; kp.fo_mom[d] = (R*)c->d_fo_mom[d].p;
-        kp.l_pos[d] = (R*)c->d_l_pos[d].p; kp.l_mom[d] = (R*)c->d_l_mom[d].p;
+        kp.x[d] = (R*)c->d_x[d].p; kp.xlo[d] = (float*)c->d_xlo[d].p; kp.p[d] = (double*)c->d_p[d].p;
+        kp.fo_pos[d] = (double*)c->d_fo_pos[d].p; kp.fo_mom[d] = (double*)c->d_fo_mom[d].p;
+        kp.l_pos[d] = (double*)c->d_l_pos[d].p; kp.l_mom[d] = (double*)c->d_l_mom[d].p;
     }
-    kp.fo_tau = (R*)c->d_fo_tau.p; kp.fo_flag = (R*)c->d_fo_flag.p;
-    kp.l_tau = (R*)c->d_l_tau.p; kp.l_T = (R*)c->d_l_T.p;
+    kp.fo_tau = (double*)c->d_fo_tau.p; kp.fo_flag = (double*)c->d_fo_flag.p;
+    kp.l_tau = (double*)c->d_l_tau.p; kp.l_T = (double*)c->d_l_T.p;
     kp.first_bad = (unsigned long long*)c->d_status.p;
     kp.rec = (double*)c->d_rec.p; kp.rec_first = c->rec_first; kp.rec_steps = c->d_rec.p ? c->rec_steps : 0;
     return LIM_OK;
@@ -298,6 +315,9 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
     const int block = block_of(c);
     const bool saving = save_every > 0 && (hist_x || hist_p);
     const int64_t end = first_step + nsteps;
+    const int64_t chunk_max = saving ? std::min<int64_t>(nsteps, save_every) : nsteps;
+    if ((rc = dev_alloc(c, c->d_steps, (size_t)std::max<int64_t>(chunk_max, 1) * step_record_bytes<R>()))) return rc;
+    kp.steps = c->d_steps.p;
     int64_t launches = 0;
     LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     int64_t s = first_step;
@@ -307,6 +327,8 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
             const int64_t next_save = ((s + save_every - 1) / save_every) * save_every;   // s >= 0
             if (next_save + 1 < chunk_end) chunk_end = next_save + 1;
         }
+        kp.step_base = s;
+        kp.step_cap = chunk_end - s;
         LIM_CUDA(c, launch_steps<R>(kp, (int)c->P.coords, s, chunk_end, block, c->stream));
         ++launches;
         const int64_t last = chunk_end - 1;
@@ -314,7 +336,7 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
             const int64_t slot = last / save_every - first_slot;
             if (slot >= 0) {
                 R* xs[3] = { kp.x[0], kp.x[1], kp.x[2] };
-                R* ps[3] = { kp.p[0], kp.p[1], kp.p[2] };
+                double* ps[3] = { kp.p[0], kp.p[1], kp.p[2] };
                 if (hist_x) {
                     LIM_CUDA(c, launch_soa_to_aos<R>(xs, sizeof(R) == 4 ? kp.xlo : nullptr, c->dims, c->n,
                                                      (double*)c->d_stage_x.p, c->stream));
@@ -322,7 +344,7 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
                                                 sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
                 }
                 if (hist_p) {
-                    LIM_CUDA(c, launch_soa_to_aos<R>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+                    LIM_CUDA(c, launch_soa_to_aos<double>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
                     LIM_CUDA(c, cudaMemcpyAsync(hist_p + slot * c->n * c->pdim, c->d_stage_p.p,
                                                 sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
                 }
@@ -349,35 +371,32 @@ int alloc_state(lim_ctx* c, int64_t n)
 {
     int rc;
     const size_t nb = (size_t)n * sizeof(R);
-    for (int d = 0; d < 3; ++d) {
-        dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
-        dev_free(c->d_fo_pos[d]); dev_free(c->d_fo_mom[d]); dev_free(c->d_l_pos[d]); dev_free(c->d_l_mom[d]);
-    }
-    dev_free(c->d_fo_tau); dev_free(c->d_fo_flag); dev_free(c->d_l_tau); dev_free(c->d_l_T);
+    // buffers are reused when large enough (dev_alloc keeps a sufficient allocation)
     if (n == 0) return LIM_OK;
     for (int d = 0; d < c->dims; ++d) {
         if ((rc = dev_alloc(c, c->d_x[d], nb))) return rc;
         if (sizeof(R) == 4 && (rc = dev_alloc(c, c->d_xlo[d], (size_t)n * sizeof(float)))) return rc;
     }
-    for (int d = 0; d < c->pdim; ++d)
-        if ((rc = dev_alloc(c, c->d_p[d], nb))) return rc;
+    for (int d = 0; d < c->pdim; ++d)     // momenta are FP64 in both precisions
+        if ((rc = dev_alloc(c, c->d_p[d], (size_t)n * sizeof(double)))) return rc;
     if (c->P.freezeout_capture) {
+        const size_t nd = (size_t)n * sizeof(double);   // the latch is FP64 in both precisions
         for (int d = 0; d < c->dims; ++d) {
-            if ((rc = dev_alloc(c, c->d_fo_pos[d], nb))) return rc;
-            if ((rc = dev_alloc(c, c->d_l_pos[d], nb))) return rc;
-            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_pos[d].p, 0, nb, c->stream));
-            LIM_CUDA(c, cudaMemsetAsync(c->d_l_pos[d].p, 0, nb, c->stream));
+            if ((rc = dev_alloc(c, c->d_fo_pos[d], nd))) return rc;
+            if ((rc = dev_alloc(c, c->d_l_pos[d], nd))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_pos[d].p, 0, nd, c->stream));
+            LIM_CUDA(c, cudaMemsetAsync(c->d_l_pos[d].p, 0, nd, c->stream));
         }
         for (int d = 0; d < c->pdim; ++d) {
-            if ((rc = dev_alloc(c, c->d_fo_mom[d], nb))) return rc;
-            if ((rc = dev_alloc(c, c->d_l_mom[d], nb))) return rc;
-            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_mom[d].p, 0, nb, c->stream));
-            LIM_CUDA(c, cudaMemsetAsync(c->d_l_mom[d].p, 0, nb, c->stream));
+            if ((rc = dev_alloc(c, c->d_fo_mom[d], nd))) return rc;
+            if ((rc = dev_alloc(c, c->d_l_mom[d], nd))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(c->d_fo_mom[d].p, 0, nd, c->stream));
+            LIM_CUDA(c, cudaMemsetAsync(c->d_l_mom[d].p, 0, nd, c->stream));
         }
         DevBuf* bufs[4] = { &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T };
         for (DevBuf* b : bufs) {
-            if ((rc = dev_alloc(c, *b, nb))) return rc;
-            LIM_CUDA(c, cudaMemsetAsync(b->p, 0, nb, c->stream));
+            if ((rc = dev_alloc(c, *b, nd))) return rc;
+            LIM_CUDA(c, cudaMemsetAsync(b->p, 0, nd, c->stream));
         }
     }
     return LIM_OK;
@@ -397,10 +416,10 @@ int upload_state_impl(lim_ctx* c, const double* x, const double* p, int64_t n)
         LIM_CUDA(c, cudaMemcpyAsync(c->d_stage_x.p, x, sizeof(double) * n * c->dims, cudaMemcpyHostToDevice, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(c->d_stage_p.p, p, sizeof(double) * n * c->pdim, cudaMemcpyHostToDevice, c->stream));
         R* xs[3] = { (R*)c->d_x[0].p, (R*)c->d_x[1].p, (R*)c->d_x[2].p };
-        R* ps[3] = { (R*)c->d_p[0].p, (R*)c->d_p[1].p, (R*)c->d_p[2].p };
+        double* ps[3] = { (double*)c->d_p[0].p, (double*)c->d_p[1].p, (double*)c->d_p[2].p };
         float* lo[3] = { (float*)c->d_xlo[0].p, (float*)c->d_xlo[1].p, (float*)c->d_xlo[2].p };
         LIM_CUDA(c, launch_aos_to_soa<R>((const double*)c->d_stage_x.p, c->dims, n, xs, sizeof(R) == 4 ? lo : nullptr, c->stream));
-        LIM_CUDA(c, launch_aos_to_soa<R>((const double*)c->d_stage_p.p, c->pdim, n, ps, nullptr, c->stream));
+        LIM_CUDA(c, launch_aos_to_soa<double>((const double*)c->d_stage_p.p, c->pdim, n, ps, nullptr, c->stream));
     }
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     c->state_prec = (int)c->P.precision;
@@ -413,14 +432,14 @@ int download_state_impl(lim_ctx* c, double* x, double* p)
 {
     if (c->n == 0) return LIM_OK;
     R* xs[3] = { (R*)c->d_x[0].p, (R*)c->d_x[1].p, (R*)c->d_x[2].p };
-    R* ps[3] = { (R*)c->d_p[0].p, (R*)c->d_p[1].p, (R*)c->d_p[2].p };
+    double* ps[3] = { (double*)c->d_p[0].p, (double*)c->d_p[1].p, (double*)c->d_p[2].p };
     float* lo[3] = { (float*)c->d_xlo[0].p, (float*)c->d_xlo[1].p, (float*)c->d_xlo[2].p };
     if (x) {
         LIM_CUDA(c, launch_soa_to_aos<R>(xs, sizeof(R) == 4 ? lo : nullptr, c->dims, c->n, (double*)c->d_stage_x.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(x, c->d_stage_x.p, sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
     }
     if (p) {
-        LIM_CUDA(c, launch_soa_to_aos<R>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+        LIM_CUDA(c, launch_soa_to_aos<double>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(p, c->d_stage_p.p, sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
     }
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -432,26 +451,26 @@ int download_fo_impl(lim_ctx* c, double* fo_pos, double* fo_mom, double* fo_tau,
 {
     if (!c->P.freezeout_capture) return fail(c, LIM_ERR_STATE, "freezeout_capture is off");
     if (c->n == 0) return LIM_OK;
-    R* fp[3] = { (R*)c->d_fo_pos[0].p, (R*)c->d_fo_pos[1].p, (R*)c->d_fo_pos[2].p };
-    R* fm[3] = { (R*)c->d_fo_mom[0].p, (R*)c->d_fo_mom[1].p, (R*)c->d_fo_mom[2].p };
-    R* ft[1] = { (R*)c->d_fo_tau.p };
-    R* ff[1] = { (R*)c->d_fo_flag.p };
+    double* fp[3] = { (double*)c->d_fo_pos[0].p, (double*)c->d_fo_pos[1].p, (double*)c->d_fo_pos[2].p };
+    double* fm[3] = { (double*)c->d_fo_mom[0].p, (double*)c->d_fo_mom[1].p, (double*)c->d_fo_mom[2].p };
+    double* ft[1] = { (double*)c->d_fo_tau.p };
+    double* ff[1] = { (double*)c->d_fo_flag.p };
     if (fo_pos) {
-        LIM_CUDA(c, launch_soa_to_aos<R>(fp, nullptr, c->dims, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, launch_soa_to_aos<double>(fp, nullptr, c->dims, c->n, (double*)c->d_stage_x.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(fo_pos, c->d_stage_x.p, sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
     }
     if (fo_mom) {
-        LIM_CUDA(c, launch_soa_to_aos<R>(fm, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
+        LIM_CUDA(c, launch_soa_to_aos<double>(fm, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(fo_mom, c->d_stage_p.p, sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
     }
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     if (fo_tau) {
-        LIM_CUDA(c, launch_soa_to_aos<R>(ft, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, launch_soa_to_aos<double>(ft, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(fo_tau, c->d_stage_x.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
         LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     }
     if (fo_flag) {
-        LIM_CUDA(c, launch_soa_to_aos<R>(ff, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
+        LIM_CUDA(c, launch_soa_to_aos<double>(ff, nullptr, 1, c->n, (double*)c->d_stage_x.p, c->stream));
         LIM_CUDA(c, cudaMemcpyAsync(fo_flag, c->d_stage_x.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
         LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     }
@@ -516,9 +535,9 @@ int lim_destroy(lim_ctx* c)
     if (!c) return LIM_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
                       &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
-                      &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec };
+                      &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -543,9 +562,9 @@ int lim_synchronize(lim_ctx* c)
 int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
 {
     if (!c || !bytes) return LIM_ERR_ARG;
-    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
                             &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
-                            &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec };
+                            &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -695,6 +714,73 @@ int lim_download_state(lim_ctx* c, double* x, double* p)
     return c->state_prec == LIM_FP32 ? download_state_impl<float>(c, x, p) : download_state_impl<double>(c, x, p);
 }
 
+namespace {
+// The buffers a checkpoint covers, with their sizes for the current state.
+int state_buffers(lim_ctx* c, DevBuf** bufs, size_t* sizes)
+{
+    int k = 0;
+    const size_t n = (size_t)c->n;
+    const size_t rb = c->state_prec == LIM_FP32 ? sizeof(float) : sizeof(double);
+    for (int d = 0; d < c->dims; ++d) {
+        bufs[k] = &c->d_x[d]; sizes[k++] = n * rb;
+        if (c->state_prec == LIM_FP32) { bufs[k] = &c->d_xlo[d]; sizes[k++] = n * sizeof(float); }
+    }
+    for (int d = 0; d < c->pdim; ++d) { bufs[k] = &c->d_p[d]; sizes[k++] = n * sizeof(double); }
+    if (c->P.freezeout_capture) {
+        for (int d = 0; d < c->dims; ++d) {
+            bufs[k] = &c->d_fo_pos[d]; sizes[k++] = n * sizeof(double);
+            bufs[k] = &c->d_l_pos[d]; sizes[k++] = n * sizeof(double);
+        }
+        for (int d = 0; d < c->pdim; ++d) {
+            bufs[k] = &c->d_fo_mom[d]; sizes[k++] = n * sizeof(double);
+            bufs[k] = &c->d_l_mom[d]; sizes[k++] = n * sizeof(double);
+        }
+        DevBuf* f[4] = { &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T };
+        for (DevBuf* b : f) { bufs[k] = b; sizes[k++] = n * sizeof(double); }
+    }
+    bufs[k] = &c->d_status; sizes[k++] = sizeof(unsigned long long);
+    return k;
+}
+}  // namespace
+
+int lim_state_save(lim_ctx* c)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "no particle state uploaded");
+    cudaSetDevice(c->device);
+    DevBuf* bufs[40];
+    size_t sizes[40];
+    const int k = state_buffers(c, bufs, sizes);
+    size_t total = 0;
+    for (int j = 0; j < k; ++j) total += (sizes[j] + 255) & ~(size_t)255;
+    int rc = dev_alloc(c, c->d_ckpt, total);
+    if (rc) return rc;
+    size_t off = 0;
+    for (int j = 0; j < k; ++j) {
+        if (sizes[j]) LIM_CUDA(c, cudaMemcpyAsync((char*)c->d_ckpt.p + off, bufs[j]->p, sizes[j], cudaMemcpyDeviceToDevice, c->stream));
+        off += (sizes[j] + 255) & ~(size_t)255;
+    }
+    c->ckpt_n = c->n;
+    return LIM_OK;
+}
+
+int lim_state_restore(lim_ctx* c)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!c->have_state || !c->d_ckpt.p || c->ckpt_n != c->n)
+        return fail(c, LIM_ERR_STATE, "no checkpoint of the current state (lim_state_save)");
+    cudaSetDevice(c->device);
+    DevBuf* bufs[40];
+    size_t sizes[40];
+    const int k = state_buffers(c, bufs, sizes);
+    size_t off = 0;
+    for (int j = 0; j < k; ++j) {
+        if (sizes[j]) LIM_CUDA(c, cudaMemcpyAsync(bufs[j]->p, (char*)c->d_ckpt.p + off, sizes[j], cudaMemcpyDeviceToDevice, c->stream));
+        off += (sizes[j] + 255) & ~(size_t)255;
+    }
+    return LIM_OK;
+}
+
 int lim_initial_lab_boost(lim_ctx* c)
 {
     if (!c) return LIM_ERR_ARG;
@@ -797,6 +883,27 @@ int lim_philox_device(lim_ctx* c, const uint32_t ctr[4], const uint32_t key[2], 
     LIM_CUDA(c, launch_philox_probe((const uint32_t*)c->d_probe.p, (uint32_t*)c->d_probe.p + 8, c->stream));
     LIM_CUDA(c, cudaMemcpyAsync(out, (uint32_t*)c->d_probe.p + 8, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    return LIM_OK;
+}
+
+int lim_probe_fma_rate(lim_ctx* c, double* thread_fma_per_s, double* ms_out)
+{
+    if (!c || !thread_fma_per_s) return LIM_ERR_ARG;
+    cudaSetDevice(c->device);
+    int nsm = 0;
+    LIM_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    const int blocks = nsm * 8, iters = 4096;
+    int rc = dev_alloc(c, c->d_probe, (size_t)blocks * 256 * sizeof(float));
+    if (rc) return rc;
+    LIM_CUDA(c, launch_fma_probe((float*)c->d_probe.p, blocks, 64, c->stream));   // warm-up
+    LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    LIM_CUDA(c, launch_fma_probe((float*)c->d_probe.p, blocks, iters, c->stream));
+    LIM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    LIM_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    LIM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *thread_fma_per_s = (double)blocks * 256.0 * iters * 64.0 / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
     return LIM_OK;
 }
 

@@ -31,6 +31,7 @@ struct MediumDev {
     const typename V2T<R>::type* TV;
     const R* V2; int use_v2;
     const double* tgd;                           // tgrid in FP64 (time cell is found in FP64)
+    const double* xgd;                           // xgrid in FP64 (FP64 freeze-out temperature)
     // analytic Bjorken T(tau) = T0 (tau0/tau)^power
     double bj_T0, bj_tau0, bj_power;
     // 2+1D grid, float4 (T, ux, uy, 0) per node, [it][iy][ix]
@@ -58,14 +59,18 @@ struct KParams {
     const R* rta;  int n_rta;  R rta_Tmin, rta_invdT;
     const R* icdf; int nU, nT; R ic_Tmin, ic_invdT;
     MediumDev<R> med;
-    // particle state, structure of arrays
-    R* x[3]; float* xlo[3]; R* p[3];
-    // freeze-out latch: outputs and the last-above cache
-    R* fo_pos[3]; R* fo_mom[3]; R* fo_tau; R* fo_flag;
-    R* l_pos[3]; R* l_mom[3]; R* l_tau; R* l_T;
+    // particle state, structure of arrays.  Momenta are accumulated in FP64 in both
+    // precisions (the FP32 path adds FP32-computed increments to an FP64 state).
+    R* x[3]; float* xlo[3]; double* p[3];
+    // freeze-out latch: outputs and the last-above cache (FP64 in both precisions:
+    // the latch divides by a one-step temperature change)
+    double* fo_pos[3]; double* fo_mom[3]; double* fo_tau; double* fo_flag;
+    double* l_pos[3]; double* l_mom[3]; double* l_tau; double* l_T;
     // status and diagnostics
     unsigned long long* first_bad;   // atomicMin of the first non-finite step
     double* rec; int64_t rec_first, rec_steps;
+    // per-step records (StepRec<R>, lim_step.cuh) for steps [step_base, step_base + step_cap)
+    void* steps; int64_t step_base, step_cap;
 };
 
 // ---------------------------------------------------------------------------
@@ -117,7 +122,8 @@ __device__ __forceinline__ R eval_spline(R T, R Tmin, R invdT, const R* __restri
     int i = fl < R(0) ? 0 : (fl > R(n - 2) ? n - 2 : (int)fl);
     R t = u - R(i);
     R y0 = __ldg(vals + i), y1 = __ldg(vals + i + 1);
-    return (R(1) - t) * y0 + t * y1;
+    if (sizeof(R) == 8) return (R(1) - t) * y0 + t * y1;   // the reference's form, for FP64 parity
+    return y0 + t * (y1 - y0);                             // FP32: no cancellation when |t| is large
 }
 
 // ---------------------------------------------------------------------------

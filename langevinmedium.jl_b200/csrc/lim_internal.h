@@ -12,6 +12,10 @@ constexpr int kObsNum = 12;   // LIM_OBS_NUM
 template <typename R>
 cudaError_t launch_steps(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st);
 
+// Bytes of one per-step record (the step table holds one per step of a launch).
+template <typename R>
+size_t step_record_bytes();
+
 // Step-0 lab boost (simulate_cpu.jl:160-163).
 template <typename R>
 cudaError_t launch_lab_boost(const KParams<R>& kp, int block, cudaStream_t st);
@@ -28,5 +32,8 @@ cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, do
                                double* partials, int64_t nblocks_max, double* out, cudaStream_t st);
 
 cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
+
+// FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.
+cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st);
 
 }  // namespace lim

@@ -12,10 +12,10 @@
 namespace lim {
 
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&x)[3], float (&xl)[3], R (&p)[3])
+__device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { x[d] = R(0); xl[d] = 0.f; p[d] = R(0); }
+    for (int d = 0; d < 3; ++d) { x[d] = R(0); xl[d] = 0.f; p[d] = 0.0; }
 #pragma unroll
     for (int d = 0; d < DIMS; ++d) {
         x[d] = kp.x[d][i];
@@ -26,7 +26,7 @@ __device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&
 }
 
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, const R (&x)[3], const float (&xl)[3], const R (&p)[3])
+__device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, const R (&x)[3], const float (&xl)[3], const double (&p)[3])
 {
 #pragma unroll
     for (int d = 0; d < DIMS; ++d) {
@@ -38,7 +38,7 @@ __device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, con
 }
 
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ bool state_finite(const R (&x)[3], const R (&p)[3])
+__device__ __forceinline__ bool state_finite(const R (&x)[3], const double (&p)[3])
 {
     bool ok = true;
 #pragma unroll
@@ -48,18 +48,27 @@ __device__ __forceinline__ bool state_finite(const R (&x)[3], const R (&p)[3])
     return ok;
 }
 
-template <typename R, int MED, int DIMS, int PDIM>
+template <typename R, int MED>
+__global__ void k_step_table(const KParams<R> kp, int64_t s0, int64_t n)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    ((StepRec<R>*)kp.steps)[k] = make_step_rec<R, MED>(kp, s0 + k);
+}
+
+template <bool REC, bool FO, typename R, int MED, int DIMS, int PDIM>
 __global__ void __launch_bounds__(256)
 k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kp.n) return;
-    R x[3], p[3];
+    R x[3];
+    double p[3];
     float xl[3];
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    R flag = R(0), ltau = R(0), lT = R(0);
-    R lpos[3] = { R(0), R(0), R(0) }, lmom[3] = { R(0), R(0), R(0) };
-    if (kp.fo_capture) {
+    double flag = 0.0, ltau = 0.0, lT = 0.0;
+    double lpos[3] = { 0.0, 0.0, 0.0 }, lmom[3] = { 0.0, 0.0, 0.0 };
+    if (FO) {
         flag = kp.fo_flag[i]; ltau = kp.l_tau[i]; lT = kp.l_T[i];
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
@@ -67,18 +76,19 @@ k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
         for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
     }
     const uint32_t pid = (uint32_t)(kp.pid_offset + i);
+    const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
     for (int64_t s = s0; s < s1; ++s) {
-        if (kp.stop_fo && flag != R(0)) break;
-        const StepU<R> su = step_uniforms<R, MED>(kp, s);
-        cart_step<R, MED, DIMS, PDIM>(kp, su, i, s, pid, x, xl, p);
-        if (kp.fo_capture) freezeout_latch<R, MED, DIMS, PDIM>(kp, su, i, x, p, flag, lpos, lmom, ltau, lT);
+        if (FO && kp.stop_fo && flag != 0.0) break;
+        const StepRec<R> sr = tab[s];
+        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, pid, x, xl, p);
+        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT);
         if (!state_finite<R, DIMS, PDIM>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
         }
     }
     store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    if (kp.fo_capture) {
+    if (FO) {
         kp.l_tau[i] = ltau; kp.l_T[i] = lT;
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos[d];
@@ -87,19 +97,21 @@ k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
     }
 }
 
-template <typename R>
+template <bool REC, typename R>
 __global__ void __launch_bounds__(256)
 k_milne(const KParams<R> kp, int64_t s0, int64_t s1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kp.n) return;
-    R x[3], p[3];
+    R x[3];
+    double p[3];
     float xl[3];
     load_state<R, 2, 2>(kp, i, x, xl, p);
     const uint32_t pid = (uint32_t)(kp.pid_offset + i);
+    const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
     for (int64_t s = s0; s < s1; ++s) {
-        const StepMilne<R> su = milne_uniforms<R>(kp, s);
-        milne_step<R>(kp, su, i, s, pid, x, xl, p);
+        const StepRec<R> sr = tab[s];
+        milne_step<REC, R>(kp, sr, i, s, pid, x, xl, p);
         if (!state_finite<R, 2, 2>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
@@ -114,12 +126,13 @@ k_lab_boost(const KParams<R> kp)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kp.n) return;
-    R x[3], p[3];
+    R x[3];
+    double p[3];
     float xl[3];
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    const StepU<R> su = step_uniforms<R, MED>(kp, 0);
-    Local<R> L = local_medium<R, MED, DIMS>(kp, su, x);
-    boost<R, DIMS, PDIM>(kp, L, p, true);
+    const StepRec<R> sr = make_step_rec<R, MED>(kp, 0);
+    const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x);
+    if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
 }
@@ -129,41 +142,74 @@ k_lab_boost(const KParams<R> kp)
 // ---------------------------------------------------------------------------
 static inline unsigned grid_of(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
-template <typename R, int MED>
-static cudaError_t launch_cart_med(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
+template <bool REC, bool FO, typename R, int MED>
+static cudaError_t launch_cart_fo(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
 {
     const unsigned g = grid_of(kp.n, block);
     const int dp = kp.dims * 10 + kp.pdim;
     if (MED == MED_GRID) {
-        if (dp == 22) k_cart<R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1);
-        else if (dp == 23) k_cart<R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1);
+        if (dp == 22) k_cart<REC, FO, R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1);
+        else if (dp == 23) k_cart<REC, FO, R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1);
         else return cudaErrorInvalidValue;
         return cudaGetLastError();
     }
     switch (dp) {
-    case 11: k_cart<R, MED, 1, 1><<<g, block, 0, st>>>(kp, s0, s1); break;
-    case 22: k_cart<R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1); break;
-    case 23: k_cart<R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
-    case 33: k_cart<R, MED, 3, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 11: k_cart<REC, FO, R, MED, 1, 1><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 22: k_cart<REC, FO, R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 23: k_cart<REC, FO, R, MED, 2, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
+    case 33: k_cart<REC, FO, R, MED, 3, 3><<<g, block, 0, st>>>(kp, s0, s1); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template <bool REC, typename R, int MED>
+static cudaError_t launch_cart_med(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
+{
+    return kp.fo_capture ? launch_cart_fo<REC, true, R, MED>(kp, s0, s1, block, st)
+                         : launch_cart_fo<REC, false, R, MED>(kp, s0, s1, block, st);
+}
+
+template <typename R, int MED>
+static cudaError_t launch_table(const KParams<R>& kp, int64_t s0, int64_t s1, cudaStream_t st)
+{
+    const int64_t n = s1 - s0;
+    k_step_table<R, MED><<<grid_of(n, 128), 128, 0, st>>>(kp, s0, n);
+    return cudaGetLastError();
+}
+
+template <bool REC, typename R>
+static cudaError_t launch_steps_rec(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st)
+{
+    cudaError_t e;
+    if (coords == 1) {
+        if ((e = launch_table<R, MED_MILNE_TABLE>(kp, s0, s1, st)) != cudaSuccess) return e;
+        k_milne<REC, R><<<grid_of(kp.n, block), block, 0, st>>>(kp, s0, s1);
+        return cudaGetLastError();
+    }
+    switch (kp.med.kind) {
+    case MED_RT:
+        if ((e = launch_table<R, MED_RT>(kp, s0, s1, st)) != cudaSuccess) return e;
+        return launch_cart_med<REC, R, MED_RT>(kp, s0, s1, block, st);
+    case MED_BJORKEN:
+        if ((e = launch_table<R, MED_BJORKEN>(kp, s0, s1, st)) != cudaSuccess) return e;
+        return launch_cart_med<REC, R, MED_BJORKEN>(kp, s0, s1, block, st);
+    case MED_GRID:
+        if ((e = launch_table<R, MED_GRID>(kp, s0, s1, st)) != cudaSuccess) return e;
+        return launch_cart_med<REC, R, MED_GRID>(kp, s0, s1, block, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 template <typename R>
 cudaError_t launch_steps(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st)
 {
     if (kp.n == 0 || s1 <= s0) return cudaSuccess;
-    if (coords == 1) {
-        k_milne<R><<<grid_of(kp.n, block), block, 0, st>>>(kp, s0, s1);
-        return cudaGetLastError();
-    }
-    switch (kp.med.kind) {
-    case MED_RT: return launch_cart_med<R, MED_RT>(kp, s0, s1, block, st);
-    case MED_BJORKEN: return launch_cart_med<R, MED_BJORKEN>(kp, s0, s1, block, st);
-    case MED_GRID: return launch_cart_med<R, MED_GRID>(kp, s0, s1, block, st);
-    }
-    return cudaErrorInvalidValue;
+    // the per-step table of this launch holds steps [s0, s1) at [0, s1 - s0)
+    if (!kp.steps || s0 != kp.step_base || s1 - s0 > kp.step_cap) return cudaErrorInvalidValue;
+    const bool rec = kp.rec != nullptr && kp.rec_steps > 0;
+    return rec ? launch_steps_rec<true, R>(kp, coords, s0, s1, block, st)
+               : launch_steps_rec<false, R>(kp, coords, s0, s1, block, st);
 }
 
 template <typename R, int MED>
@@ -265,7 +311,7 @@ k_obs_partials(const KParams<R> kp, int from_fo, double cut, double width, doubl
         bool use = true;
         double p[3] = { 0, 0, 0 }, x[3] = { 0, 0, 0 };
         if (from_fo) {
-            use = kp.fo_flag[i] != R(0);
+            use = kp.fo_flag[i] != 0.0;
             for (int d = 0; d < kp.pdim; ++d) p[d] = (double)kp.fo_mom[d][i];
             for (int d = 0; d < kp.dims; ++d) x[d] = (double)kp.fo_pos[d][i];
         } else {
@@ -336,6 +382,28 @@ cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, do
     return cudaGetLastError();
 }
 
+// FP32 FMA issue-rate probe: 8 independent dependency chains per thread.
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, int iters, float b, float c)
+{
+    float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+    float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            a0 = fmaf(a0, b, c); a1 = fmaf(a1, b, c); a2 = fmaf(a2, b, c); a3 = fmaf(a3, b, c);
+            a4 = fmaf(a4, b, c); a5 = fmaf(a5, b, c); a6 = fmaf(a6, b, c); a7 = fmaf(a7, b, c);
+        }
+    }
+    float s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st)
+{
+    k_fma_probe<<<blocks, 256, 0, st>>>(out, iters, 0.99999f, 1e-6f);
+    return cudaGetLastError();
+}
+
 __global__ void k_philox_probe(const uint32_t* ck, uint32_t* out)
 {
     uint4 r = philox4x32_10(make_uint4(ck[0], ck[1], ck[2], ck[3]), make_uint2(ck[4], ck[5]));
@@ -348,7 +416,12 @@ cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStre
     return cudaGetLastError();
 }
 
+template <typename R>
+size_t step_record_bytes() { return sizeof(StepRec<R>); }
+
 // explicit instantiations
+template size_t step_record_bytes<double>();
+template size_t step_record_bytes<float>();
 template cudaError_t launch_steps<double>(const KParams<double>&, int, int64_t, int64_t, int, cudaStream_t);
 template cudaError_t launch_steps<float>(const KParams<float>&, int, int64_t, int64_t, int, cudaStream_t);
 template cudaError_t launch_lab_boost<double>(const KParams<double>&, int, cudaStream_t);

@@ -5,76 +5,99 @@
 //   | OU kick + RTA} -> lab boost -> streaming (+diffusion, reflection)
 // fused into one device function so that the state never leaves registers.
 // Medium time at step s is s*dt + t0 (kernels_cpu.jl:67).
+//
+// Variates per step (counter-based Philox, see lim_common.cuh), slot numbers as
+// recorded by the noise-recording mode:
+//   group MOM  u0..u3: momentum normals (u0,u1)->(xi0,xi1), (u2,u3)->(xi2,z3);
+//                      RTA decision u_collide = Phi(z3) when pdim = 3, u2 when
+//                      pdim < 3, u0 in pure RTA mode                   [slots 0-3]
+//   group RTA  (drawn only when a collision happens): u_sample = u0,
+//                      (u1,u2) -> directions g0, g1                    [slots 4-6]
+//   group RTADIR (pdim = 3 collisions): (u0,u1) -> g2                  [slot 7]
+//   group DIFF position-diffusion normals                              [slots 8-10]
 #pragma once
 #include "lim_common.cuh"
 
 namespace lim {
 
-// Per-step values that are the same for every particle.
+// ---------------------------------------------------------------------------
+// Per-step record, identical for every particle: computed once per launch by
+// k_step_table and read by every thread with one broadcast load.
+// ---------------------------------------------------------------------------
 template <typename R>
-struct StepU {
-    double t;        // medium time s*dt + t0
-    R tR;
-    int kt; R wt;    // (r,t) table: time cell and weight
-    R T_bj;          // Bjorken temperature at t
-    int it; R wtg;       // grid: time cell and weight
+struct __align__(16) StepRec {
+    double t;    // medium time s*dt + t0
+    R tR;        // the same in R
+    R wt;        // time weight of the (r,t) table, the grid or the Milne table
+    R T_bj;      // Bjorken temperature at t
+    R zf;        // Bjorken redshift factor tau_a/(tau_a+dt), 1 when not applied
+    int kt;      // time cell
+    int pad;
+    double wtd;  // time weight in FP64
+    double Td;   // Bjorken temperature in FP64
 };
 
+enum { MED_MILNE_TABLE = 3 };   // Milne (tau, r): unclamped time interpolation
+
 template <typename R, int MED>
-__device__ __forceinline__ StepU<R> step_uniforms(const KParams<R>& kp, int64_t s)
+__device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_t s)
 {
-    StepU<R> u;
+    StepRec<R> u;
     u.t = __dadd_rn(__dmul_rn((double)s, kp.dt), kp.t0);
     u.tR = (R)u.t;
-    u.kt = 0; u.wt = R(0); u.T_bj = R(0); u.it = 0; u.wtg = R(0);
+    u.kt = 0; u.pad = 0; u.wt = R(0); u.T_bj = R(0); u.zf = R(1); u.wtd = 0.0; u.Td = 0.0;
     const MediumDev<R>& md = kp.med;
-    if (MED == MED_RT) {
+    if (MED == MED_RT || MED == MED_MILNE_TABLE) {
         const double* tg = md.tgd;
-        int nt = md.nt;
-        double tq = u.t > tg[nt - 1] ? tg[nt - 1] : (u.t < tg[0] ? tg[0] : u.t);
-        int k;
-        if (md.t_uniform) {
-            double f = (tq - md.tg0) * md.tinvd;
-            k = f > 0.0 ? (int)f : 0;
-            k = k > nt - 1 ? nt - 1 : k;
-            while (k + 1 < nt && __ldg(tg + k + 1) <= tq) ++k;
-            while (k > 0 && __ldg(tg + k) > tq) --k;
-        } else {
-            int lo = -1, hi = nt;
-            while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (__ldg(tg + mid) <= tq) lo = mid; else hi = mid; }
-            k = lo < 0 ? 0 : lo;
-        }
+        const int nt = md.nt;
+        const bool clamp = MED == MED_RT;
+        double tq = u.t;
+        if (clamp) tq = tq > tg[nt - 1] ? tg[nt - 1] : (tq < tg[0] ? tg[0] : tq);
+        int lo = -1, hi = nt;          // last node <= tq (searchsortedlast)
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (tg[mid] <= tq) lo = mid; else hi = mid; }
+        int k = lo < 0 ? 0 : lo;
         k = k > nt - 2 ? nt - 2 : k;
-        double y0 = __ldg(tg + k), y1 = __ldg(tg + k + 1), dy = y1 - y0;
+        double y0 = tg[k], y1 = tg[k + 1], dy = y1 - y0;
         u.kt = k;
-        u.wt = (R)(fabs(dy) < kEps ? 0.0 : (tq - y0) / dy);
+        if (clamp) u.wtd = fabs(dy) < kEps ? 0.0 : (tq - y0) / dy;      // kernels_cpu.jl:45
+        else u.wtd = (tq - y0) / dy;                                     // kernels_cpu_GC.jl:51
+        u.wt = (R)u.wtd;
     } else if (MED == MED_BJORKEN) {
         double T = (u.t > md.bj_tau0) ? md.bj_T0 * pow(md.bj_tau0 / u.t, md.bj_power) : md.bj_T0;
         u.T_bj = (R)T;
+        u.Td = T;
     } else {
         double tq = u.t > md.gtl ? md.gtl : (u.t < md.gt0 ? md.gt0 : u.t);
         double f = (tq - md.gt0) / md.gdt_d;
         double fl = floor(f);
         int it = fl < 0.0 ? 0 : (fl > (double)(md.gnt - 2) ? md.gnt - 2 : (int)fl);
-        u.it = it;
-        u.wtg = (R)(f - (double)it);
+        u.kt = it;
+        u.wtd = f - (double)it;
+        u.wt = (R)u.wtd;
+    }
+    if (kp.redshift) {                 // kernels_cpu.jl:427-435
+        double ta = kp.t0 + (double)(s - 1) * kp.dt;
+        if (ta > 0.0) u.zf = (R)(ta / (ta + kp.dt));
     }
     return u;
 }
 
-// (r, t) table: bilinear interpolation of (T, V) at radius r (clamped), time cell from StepU.
+// ---------------------------------------------------------------------------
+// medium lookups
+// ---------------------------------------------------------------------------
+// (r, t) table: bilinear interpolation of (T, V) at radius r (clamped).
 template <typename R>
-__device__ __forceinline__ void rt_lookup(const MediumDev<R>& md, const StepU<R>& su, R r, R& T, R& V)
+__device__ __forceinline__ void rt_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R r, R& T, R& V)
 {
     R rq = jclamp(r, __ldg(md.xg), __ldg(md.xg + md.nr - 1));
     int i = cell_index(md.xg, md.nr, rq, md.x_uniform, md.xg0, md.xinvd);
     R x0 = __ldg(md.xg + i), x1 = __ldg(md.xg + i + 1);
     R dx = x1 - x0;
     R xd = fabs(dx) < R(kEps) ? R(0) : (rq - x0) / dx;
-    const int nr = md.nr, j = su.kt;
+    const int nr = md.nr, j = sr.kt;
     auto a00 = md.TV[i + nr * j],       a10 = md.TV[i + 1 + nr * j];
     auto a01 = md.TV[i + nr * (j + 1)], a11 = md.TV[i + 1 + nr * (j + 1)];
-    R yd = su.wt;
+    R yd = sr.wt;
     R c0 = a00.x * (R(1) - xd) + a10.x * xd;
     R c1 = a01.x * (R(1) - xd) + a11.x * xd;
     T = c0 * (R(1) - yd) + c1 * yd;
@@ -84,17 +107,17 @@ __device__ __forceinline__ void rt_lookup(const MediumDev<R>& md, const StepU<R>
 }
 
 template <typename R>
-__device__ __forceinline__ R rt_lookup_scalar(const MediumDev<R>& md, const StepU<R>& su, const R* __restrict__ vals, R r)
+__device__ __forceinline__ R rt_lookup_scalar(const MediumDev<R>& md, const StepRec<R>& sr, const R* __restrict__ vals, R r)
 {
     R rq = jclamp(r, __ldg(md.xg), __ldg(md.xg + md.nr - 1));
     int i = cell_index(md.xg, md.nr, rq, md.x_uniform, md.xg0, md.xinvd);
     R x0 = __ldg(md.xg + i), x1 = __ldg(md.xg + i + 1);
     R dx = x1 - x0;
     R xd = fabs(dx) < R(kEps) ? R(0) : (rq - x0) / dx;
-    const int nr = md.nr, j = su.kt;
+    const int nr = md.nr, j = sr.kt;
     R v00 = __ldg(vals + i + nr * j), v10 = __ldg(vals + i + 1 + nr * j);
     R v01 = __ldg(vals + i + nr * (j + 1)), v11 = __ldg(vals + i + 1 + nr * (j + 1));
-    R yd = su.wt;
+    R yd = sr.wt;
     R c0 = v00 * (R(1) - xd) + v10 * xd;
     R c1 = v01 * (R(1) - xd) + v11 * xd;
     return c0 * (R(1) - yd) + c1 * yd;
@@ -118,13 +141,13 @@ __device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, in
 }
 
 template <typename R>
-__device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepU<R>& su, R xq, R yq, R& T, R& ux, R& uy)
+__device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R xq, R yq, R& T, R& ux, R& uy)
 {
     int ix, iy;
     R Wx, Wy;
     grid_cell(md, xq, yq, ix, iy, Wx, Wy);
-    const R Wt = su.wtg;
-    const float4* s0 = md.G + ((size_t)su.it * md.gny + iy) * md.gnx + ix;
+    const R Wt = sr.wt;
+    const float4* s0 = md.G + ((size_t)sr.kt * md.gny + iy) * md.gnx + ix;
     const float4* s1 = s0 + (size_t)md.gny * md.gnx;
     float4 a00 = __ldg(s0), a10 = __ldg(s0 + 1), a01 = __ldg(s0 + md.gnx), a11 = __ldg(s0 + md.gnx + 1);
     float4 b00 = __ldg(s1), b10 = __ldg(s1 + 1), b01 = __ldg(s1 + md.gnx), b11 = __ldg(s1 + md.gnx + 1);
@@ -141,101 +164,161 @@ __device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepU<
 }
 
 // Flow seen by one particle this step: boost direction (nx, ny), signed speed v,
-// and the local temperature T at the same point.
+// the local temperature T at the same point, and whether the frame changes.
 template <typename R>
 struct Local {
     R T, v, nx, ny;
-    bool active;      // false => no boost (r < eps, kernels_cpu.jl:75-77)
+    bool boost;   // false: r < eps (kernels_cpu.jl:75-77), or FP32 with zero flow
 };
 
 template <typename R, int MED, int DIMS>
-__device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepU<R>& su, const R (&x)[3])
+__device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3])
 {
+    constexpr bool fp32 = sizeof(R) == 4;
     Local<R> L;
-    L.nx = R(0); L.ny = R(0);
+    L.nx = R(0); L.ny = R(0); L.v = R(0);
     if (MED == MED_GRID) {
         R ux, uy;
-        grid_lookup(kp.med, su, x[0], x[1], L.T, ux, uy);
+        grid_lookup(kp.med, sr, x[0], x[1], L.T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
-        L.active = !(u < R(kEps));
+        L.boost = !(u < R(kEps));
         L.v = u;
-        if (L.active) { L.nx = ux / u; L.ny = uy / u; }
+        if (L.boost) { L.nx = ux / u; L.ny = uy / u; }
+    } else if (MED == MED_BJORKEN && fp32) {
+        // zero flow: in FP32 the boost is the identity (gamma(0) rounds to 1)
+        L.T = sr.T_bj;
+        L.boost = false;
     } else {
         R r2 = R(0);
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
         R r = sqrt(r2);
-        L.active = !(r < R(kEps));
+        L.boost = !(r < R(kEps));
         if (MED == MED_RT) {
-            rt_lookup(kp.med, su, r, L.T, L.v);
-            if (DIMS >= 2 && kp.med.use_v2 && L.active) {
-                R v2m = rt_lookup_scalar(kp.med, su, kp.med.V2, r);
+            rt_lookup(kp.med, sr, r, L.T, L.v);
+            if (DIMS >= 2 && kp.med.use_v2 && L.boost) {
+                R v2m = rt_lookup_scalar(kp.med, sr, kp.med.V2, r);
                 R phi = atan2(x[1], x[0]);
                 L.v *= (R(1) + R(2) * v2m * cos(R(2) * (phi - kp.psi2)));
             }
         } else {
-            L.T = su.T_bj;
-            L.v = R(0);
+            L.T = sr.T_bj;
         }
-        if (DIMS >= 2 && L.active) { L.nx = x[0] / r; L.ny = x[1] / r; }
+        // FP64 keeps the reference's gamma(0) = 1/sqrt(1+1e-10) factor at zero flow;
+        // in FP32 that factor is 1 and the boost is skipped.
+        if (fp32 && L.v == R(0)) L.boost = false;
+        if (DIMS >= 2 && L.boost) { L.nx = x[0] / r; L.ny = x[1] / r; }
     }
     if (kp.med.T_scale != R(1)) L.T *= kp.med.T_scale;
     return L;
 }
 
-// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).
+// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  The frame
+// change is evaluated in FP64 in both precisions: with the momentum held in FP64,
+// p_par - v E does not lose the LRF momentum to cancellation at large gamma.
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, R (&p)[3], bool to_lab)
+__device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, double (&p)[3], bool to_lab)
 {
-    if (!L.active) return;
-    const R m = kp.m;
-    R v = L.v;
+    const double m = (double)kp.m;
+    double v = (double)L.v;
+    const double nx = (double)L.nx, ny = (double)L.ny;
     if (!kp.rel) {                     // Galilean p_par -/+ m v
-        R mv = m * v;
+        double mv = m * v;
         if (DIMS == 1) { p[0] = to_lab ? p[0] + mv : p[0] - mv; }
         else {
-            R dx = mv * L.nx, dy = mv * L.ny;
+            double dx = mv * nx, dy = mv * ny;
             p[0] = to_lab ? p[0] + dx : p[0] - dx;
             p[1] = to_lab ? p[1] + dy : p[1] - dy;
         }
         return;
     }
-    const R vmax = sizeof(R) == 8 ? R(0.9999999999995) : R(0.99999994f);   // sqrt(1 - 1e-12)
+    const double vmax = 0.9999999999995;   // sqrt(1 - 1e-12)
     v = jclamp(v, -vmax, vmax);
-    R gam;
-    if (sizeof(R) == 8) gam = R(1) / sqrt(R(1) - v * v + R(1e-10));
-    else gam = rsqrt((R(1) - v) * (R(1) + v) + R(1e-10));
-    R p2 = R(0);
+    double gam = 1.0 / sqrt(1.0 - v * v + 1e-10);
+    double p2 = 0.0;
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) p2 += p[d] * p[d];
-    R E = sqrt(p2 + m * m);
-    R vE = to_lab ? v * E : -(v * E);
+    double E = sqrt(p2 + m * m);
+    double vE = to_lab ? v * E : -(v * E);
     if (DIMS == 1) { p[0] = gam * (p[0] + vE); return; }
-    R px = p[0], py = p[1];
-    R ppar = px * L.nx + py * L.ny;
-    R pperpx = px - ppar * L.nx;
-    R pperpy = py - ppar * L.ny;
-    R pnew = gam * (ppar + vE);
-    p[0] = pnew * L.nx + pperpx;
-    p[1] = pnew * L.ny + pperpy;
+    double px = p[0], py = p[1];
+    double ppar = px * nx + py * ny;
+    double pperpx = px - ppar * nx;
+    double pperpy = py - ppar * ny;
+    double pnew = gam * (ppar + vE);
+    p[0] = pnew * nx + pperpx;
+    p[1] = pnew * ny + pperpy;
 }
 
-// Records the variates consumed by the step when noise recording is on.
-template <typename R>
+// Records a consumed variate (noise-recording instantiation only).
+template <bool REC, typename R>
 __device__ __forceinline__ void rec_slot(const KParams<R>& kp, int64_t s, int64_t i, int slot, R val)
 {
-    if (kp.rec && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
+    if (REC && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
         kp.rec[((s - kp.rec_first) * kNoiseSlots + slot) * kp.n + i] = (double)val;
+}
+
+// expm1(-x) for x >= 0: Taylor series below 0.05 (truncation < 1e-11 relative),
+// the library function above.
+__device__ __forceinline__ float expm1_neg(float x)
+{
+    if (x < 0.05f) {
+        float p = 1.0f / 720.0f;
+        p = fmaf(p, -x, 1.0f / 120.0f);
+        p = fmaf(p, -x, 1.0f / 24.0f);
+        p = fmaf(p, -x, 1.0f / 6.0f);
+        p = fmaf(p, -x, 0.5f);
+        p = fmaf(p, -x, 1.0f);
+        return -x * p;
+    }
+    return expm1f(-x);
 }
 
 // kernels_cpu.jl:246-357 + :406-417: exact-OU drag and kick in the LRF.
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, R (&p)[3], const R (&xi)[3])
+__device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, double (&p)[3], const R (&xi)[3])
 {
     const R M = kp.m, dt = kp.dtR;
     const R DsT_safe = kp.DsT <= R(0) ? R(0) : kp.DsT;
     R tau = DsT_safe == R(0) ? R(0) : eval_spline(T, kp.drag_Tmin, kp.drag_invdT, kp.drag, kp.n_drag);
     const bool ok = tau > R(0) && isfinite(tau);
+    if (sizeof(R) == 4) {
+        // FP32: with kappa = 2MT/tau and eta_eff = (M/E)/tau the kick amplitude
+        // sqrt(dt) kT sqrt((1-a^2)/(2 eta_eff dt)) is sqrt(T E (1-a^2)) (M in place of E
+        // when non-relativistic); a - 1 and 1 - a^2 come from one expm1 (no
+        // cancellation).  The FP32 increment is added to the FP64 momentum.
+        if (!ok) return;                                   // kT = 0: no drag, no kick
+        R pf[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pf[d] = (R)p[d];
+        if (DIMS == 1) {
+            R E = sqrt(pf[0] * pf[0] + M * M);
+            R eff = kp.rel ? M / (E * tau) : R(1) / tau;
+            R kT = sqrt((R(2) * M * T) / tau);
+            p[0] += (double)(-eff * pf[0] * dt + kp.sqrt_dt * (kT * xi[0]));
+            return;
+        }
+        R p2 = R(0);
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) p2 += pf[d] * pf[d];
+        R E = sqrt(p2 + M * M);
+        R Ew = kp.rel ? E : M;
+        if (kp.integrator == 1) {
+            R a_half = R(1) + expm1_neg((M / (Ew * tau)) * (R(0.5) * dt));
+            R p2m = R(0);
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) { R q = a_half * pf[d]; p2m += q * q; }
+            R Em = sqrt(p2m + M * M);
+            Ew = kp.rel ? Em : M;
+        }
+        R x = (M / (Ew * tau)) * dt;                         // eta_eff * dt
+        R em1 = expm1_neg(x);
+        R one_m_a2 = -em1 * (R(2) + em1);
+        R amp = (dt > R(0) && x > R(0)) ? sqrt(T * Ew * one_m_a2) : R(0);
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) p[d] += (double)(em1 * pf[d] + amp * xi[d]);
+        return;
+    }
     R etaD = ok ? R(1) / tau : R(0);
     R kappa = ok ? (R(2) * M * T) / tau : R(0);
     R kT = sqrt(kappa);
@@ -260,24 +343,14 @@ __device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, R (&p)[
         R a_half = exp(-eff * (R(0.5) * dt));
         R p2m = R(0);
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) { R pm = a_half * p[d]; p2m += pm * pm; }
+        for (int d = 0; d < PDIM; ++d) { R q = a_half * p[d]; p2m += q * q; }
         R Em = sqrt(p2m + M * M);
         eff = kp.rel ? etaD * M / Em : etaD;
     }
-    if (sizeof(R) == 8) {
-        R a = exp(-eff * dt);
-        R np = (dt > R(0) && eff > R(0)) ? kT * sqrt((R(1) - a * a) / (R(2) * eff * dt)) : R(0);
+    R a = exp(-eff * dt);
+    R np = (dt > R(0) && eff > R(0)) ? kT * sqrt((R(1) - a * a) / (R(2) * eff * dt)) : R(0);
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) p[d] += (a - R(1)) * p[d] + kp.sqrt_dt * (np * xi[d]);
-    } else {
-        // FP32: a - 1 and 1 - a^2 from one expm1 (no cancellation); the noise
-        // amplitude sqrt(dt)*kT*sqrt((1-a^2)/(2 eff dt)) = sqrt(kappa (1-a^2) / (2 eff)).
-        R em1 = expm1(-eff * dt);
-        R one_m_a2 = -em1 * (R(2) + em1);
-        R amp = (dt > R(0) && eff > R(0)) ? sqrt(kappa * one_m_a2 / (R(2) * eff)) : R(0);
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) p[d] += em1 * p[d] + amp * xi[d];
-    }
+    for (int d = 0; d < PDIM; ++d) p[d] += (a - R(1)) * p[d] + kp.sqrt_dt * (np * xi[d]);
 }
 
 // kernels_gpu.jl:88-117
@@ -290,6 +363,9 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, R u, R T)
     int iu = (int)floor(fu);
     iu = iu < 0 ? 0 : (iu > nU - 2 ? nU - 2 : iu);
     R tu = fu - R(iu);
+    // FP32: u*(nU-1) rounds away up to 2^-24 (nU-1) of the cell weight, which the steep
+    // tail of p*(u) turns into a 1e-5 error; the FMA residual restores it exactly.
+    if (sizeof(R) == 4) tu += fma(uu, R(nU - 1), -fu);
     R fT = (T - kp.ic_Tmin) * kp.ic_invdT;
     R flT = floor(fT);
     int jT = flT < R(0) ? 0 : (flT > R(nT - 2) ? nT - 2 : (int)flT);
@@ -303,79 +379,79 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, R u, R T)
     return c0 * (R(1) - tT) + c1 * tT;
 }
 
-// kernels_gpu.jl:653-704 with Philox variates (tag RTA: u_collide, u_sample, g0, g1;
-// tag RTADIR: g2).  Returns true when the particle was resampled.
-template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ bool rta_collide(const KParams<R>& kp, int64_t i, int64_t s, uint32_t pid,
-                                            R T, R (&p)[3])
+// kernels_gpu.jl:653-704: with probability Pcol = clamp(dt/tau, 0, 1) re-draw |p*|
+// from the Jüttner inverse CDF and an isotropic direction.  The collision
+// uniform u_collide comes with the step's momentum variates; the sample and the
+// direction are drawn only when the particle collides.
+template <bool REC, typename R, int DIMS, int PDIM>
+__device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, uint32_t pid,
+                                            R T, R uc, double (&p)[3])
 {
-    Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_RTA);
-    rec_slot(kp, s, i, 3, u.u[0]);
-    rec_slot(kp, s, i, 4, u.u[1]);
     R tn = (kp.DsT > R(0) && T > R(0)) ? eval_spline(T, kp.rta_Tmin, kp.rta_invdT, kp.rta, kp.n_rta) : R(0);
     R Pcol = (tn > R(0) && isfinite(tn)) ? jclamp(kp.dtR / tn, R(0), R(1)) : R(1);
-    if (!(u.u[0] < Pcol)) return false;
-    R pstar = invcdf_lookup(kp, u.u[1], T);
+    if (!(uc < Pcol || Pcol >= R(1))) return;
+    Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_RTA);
+    R pstar = invcdf_lookup(kp, u.u[0], T);
     R g[3];
-    box_muller(u.u[2], u.u[3], g[0], g[1]);
+    box_muller(u.u[1], u.u[2], g[0], g[1]);
     g[2] = R(0);
     if (PDIM == 3) {
         Uni4<R> w = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_RTADIR);
         R z;
         box_muller(w.u[0], w.u[1], g[2], z);
     }
+    rec_slot<REC>(kp, s, i, 4, u.u[0]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) rec_slot(kp, s, i, 5 + d, g[d]);
-    if (DIMS == 1) { p[0] = (g[0] < R(0) ? R(-1) : R(1)) * pstar; return true; }
+    for (int d = 0; d < 3; ++d) rec_slot<REC>(kp, s, i, 5 + d, g[d]);
+    if (DIMS == 1) { p[0] = (double)((g[0] < R(0) ? R(-1) : R(1)) * pstar); return; }
     R nrm2 = R(0);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) nrm2 += g[d] * g[d];
     R inv = pstar / sqrt(nrm2 > R(1e-300) ? nrm2 : R(1e-300));
 #pragma unroll
-    for (int d = 0; d < PDIM; ++d) p[d] = g[d] * inv;
-    return true;
+    for (int d = 0; d < PDIM; ++d) p[d] = (double)(g[d] * inv);
 }
 
 // kernels_cpu.jl:671-735 (momentum_langevin = false or DsT == 0).
 template <typename R, int MED, int DIMS>
-__device__ __forceinline__ void set_to_fluid(const KParams<R>& kp, const StepU<R>& su, const R (&x)[3], R (&p)[3])
+__device__ __forceinline__ void set_to_fluid(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3], double (&p)[3])
 {
     const R m = kp.m;
     const R vmax = sizeof(R) == 8 ? R(0.9999999999995) : R(0.99999994f);
     if (MED == MED_GRID) {
         R T, ux, uy;
-        grid_lookup(kp.med, su, x[0], x[1], T, ux, uy);
+        grid_lookup(kp.med, sr, x[0], x[1], T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
-        if (u < R(kEps)) { p[0] = R(0); p[1] = R(0); return; }
+        if (u < R(kEps)) { p[0] = 0.0; p[1] = 0.0; return; }
         R vc = kp.rel ? jclamp(u, -vmax, vmax) : u;
         R g = kp.rel ? R(1) / sqrt(R(1) - vc * vc + R(1e-10)) : R(1);
-        p[0] = m * g * vc * (ux / u);
-        p[1] = m * g * vc * (uy / u);
+        p[0] = (double)(m * g * vc * (ux / u));
+        p[1] = (double)(m * g * vc * (uy / u));
         return;
     }
     R r = DIMS == 1 ? x[0] : sqrt(x[0] * x[0] + x[1] * x[1]);
     if (r < R(kEps)) return;
     R v = R(0);
-    if (MED == MED_RT) { R Tdummy; rt_lookup(kp.med, su, r, Tdummy, v); }
+    if (MED == MED_RT) { R Tdummy; rt_lookup(kp.med, sr, r, Tdummy, v); }
     if (!kp.rel) {
-        if (DIMS == 1) p[0] = m * v;
-        else { p[0] = m * v * (x[0] / r); p[1] = m * v * (x[1] / r); }
+        if (DIMS == 1) p[0] = (double)(m * v);
+        else { p[0] = (double)(m * v * (x[0] / r)); p[1] = (double)(m * v * (x[1] / r)); }
         return;
     }
     v = jclamp(v, -vmax, vmax);
     R gam = R(1) / sqrt(R(1) - v * v + R(1e-10));
-    if (DIMS == 1) p[0] = m * gam * v;
-    else { p[0] = m * gam * v * (x[0] / r); p[1] = m * gam * v * (x[1] / r); }
+    if (DIMS == 1) p[0] = (double)(m * gam * v);
+    else { p[0] = (double)(m * gam * v * (x[0] / r)); p[1] = (double)(m * gam * v * (x[1] / r)); }
 }
 
 // Temperature at an arbitrary point of this step (diffusion, freeze-out).
 template <typename R, int MED, int DIMS>
-__device__ __forceinline__ R temperature_at(const KParams<R>& kp, const StepU<R>& su, const R (&x)[3], R r)
+__device__ __forceinline__ R temperature_at(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3], R r)
 {
     R T;
-    if (MED == MED_RT) { R V; rt_lookup(kp.med, su, r, T, V); }
-    else if (MED == MED_BJORKEN) T = su.T_bj;
-    else { R ux, uy; grid_lookup(kp.med, su, x[0], x[1], T, ux, uy); }
+    if (MED == MED_RT) { R V; rt_lookup(kp.med, sr, r, T, V); }
+    else if (MED == MED_BJORKEN) T = sr.T_bj;
+    else { R ux, uy; grid_lookup(kp.med, sr, x[0], x[1], T, ux, uy); }
     if (kp.med.T_scale != R(1)) T *= kp.med.T_scale;
     return T;
 }
@@ -395,30 +471,33 @@ __device__ __forceinline__ void acc_add(R& hi, float& lo, R dx)
 }
 
 // kernels_cpu.jl:510-637
-template <typename R, int MED, int DIMS, int PDIM>
-__device__ __forceinline__ void stream_positions(const KParams<R>& kp, const StepU<R>& su, int64_t i, int64_t s,
-                                                 uint32_t pid, R (&x)[3], float (&xl)[3], R (&p)[3])
+template <bool REC, typename R, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void stream_positions(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
+                                                 uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
     const R m = kp.m, dt = kp.dtR;
+    R pr_[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) pr_[d] = (R)p[d];
     R E2 = m * m;
 #pragma unroll
-    for (int d = 0; d < PDIM; ++d) E2 += p[d] * p[d];
+    for (int d = 0; d < PDIM; ++d) E2 += pr_[d] * pr_[d];
     R E = kp.rel ? sqrt(E2) : m;
     const R r_max = kp.med.r_max, r_axis_eps = kp.med.r_axis_eps;
     if (DIMS == 1) {
-        R r = x[0], pr = p[0];
+        R r = x[0], pr = pr_[0];
         R r_abs = fabs(r);
         R r_safe = r_abs < r_axis_eps ? r_axis_eps : r_abs;
         R dr = (pr / E) * dt;
         if (kp.diffusion) {
             R xs[3] = { r_safe, R(0), R(0) };
-            R T = temperature_at<R, MED, DIMS>(kp, su, xs, r_safe);
+            R T = temperature_at<R, MED, DIMS>(kp, sr, xs, r_safe);
             R D = (kp.DsT / (T != T ? T : (T > R(kEps) ? T : R(kEps)))) / R(kFmGeV);
             if (D > R(0)) {
                 Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_DIFF);
                 R z0, z1;
                 box_muller(u.u[0], u.u[1], z0, z1);
-                rec_slot(kp, s, i, 8, z0);
+                rec_slot<REC>(kp, s, i, 8, z0);
                 dr += (D / r_safe) * dt + sqrt(R(2) * D * dt) * z0;
             }
         }
@@ -435,14 +514,14 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
     R invE = R(1) / E;
 #pragma unroll
     for (int d = 0; d < DIMS; ++d) {
-        R dx = sizeof(R) == 8 ? dt * p[d] / E : (dt * p[d]) * invE;
+        R dx = sizeof(R) == 8 ? dt * pr_[d] / E : (dt * pr_[d]) * invE;
         acc_add(x[d], xl[d], dx);
     }
     if (kp.diffusion) {
         R r2 = R(0);
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
-        R T = temperature_at<R, MED, DIMS>(kp, su, x, sqrt(r2));
+        R T = temperature_at<R, MED, DIMS>(kp, sr, x, sqrt(r2));
         R D = (kp.DsT / (T != T ? T : (T > R(kEps) ? T : R(kEps)))) / R(kFmGeV);
         if (D > R(0)) {
             R sg = sqrt(R(2) * D * dt);
@@ -451,7 +530,7 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
             box_muller(u.u[0], u.u[1], z[0], z[1]);
             box_muller(u.u[2], u.u[3], z[2], z[3]);
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) { rec_slot(kp, s, i, 8 + d, z[d]); acc_add(x[d], xl[d], sg * z[d]); }
+            for (int d = 0; d < DIMS; ++d) { rec_slot<REC>(kp, s, i, 8 + d, z[d]); acc_add(x[d], xl[d], sg * z[d]); }
         }
     }
     if (kp.reflect && r_max > R(0)) {
@@ -463,9 +542,9 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
             R invr = R(1) / (r_now > r_axis_eps ? r_now : r_axis_eps);
             R ppar = R(0);
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) ppar += p[d] * (x[d] * invr);
+            for (int d = 0; d < DIMS; ++d) ppar += pr_[d] * (x[d] * invr);
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) p[d] -= R(2) * ppar * (x[d] * invr);
+            for (int d = 0; d < DIMS; ++d) p[d] -= (double)(R(2) * ppar * (x[d] * invr));
             R scale = (R(2) * r_max - r_now) * invr;
 #pragma unroll
             for (int d = 0; d < DIMS; ++d) { x[d] = (R)((double)x[d] + (double)xl[d]) * scale; xl[d] = 0.f; }
@@ -473,77 +552,142 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
     }
 }
 
-// Momentum noise: 4 normals from one uniform group (the first PDIM are used).
-template <typename R, int PDIM>
-__device__ __forceinline__ void momentum_noise(const KParams<R>& kp, int64_t i, int64_t s, uint32_t pid, R (&xi)[3])
-{
-    Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_MOM);
-    R z1;
-    box_muller(u.u[0], u.u[1], xi[0], xi[1]);
-    if (PDIM == 3) box_muller(u.u[2], u.u[3], xi[2], z1);
-    else xi[2] = R(0);
-#pragma unroll
-    for (int d = 0; d < PDIM; ++d) rec_slot(kp, s, i, d, xi[d]);
-}
-
 // One Cartesian step (simulate_cpu.jl:215-290).
-template <typename R, int MED, int DIMS, int PDIM>
-__device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepU<R>& su, int64_t i, int64_t s,
-                                          uint32_t pid, R (&x)[3], float (&xl)[3], R (&p)[3])
+template <bool REC, typename R, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
+                                          uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
-    Local<R> L = local_medium<R, MED, DIMS>(kp, su, x);
-    boost<R, DIMS, PDIM>(kp, L, p, false);
-    if (PDIM == 3 && kp.redshift) {
-        double ta = kp.t0 + (double)(s - 1) * kp.dt;
-        if (ta > 0.0) p[2] *= (R)(ta / (ta + kp.dt));
-    }
+    const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x);
+    if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, false);
+    if (PDIM == 3 && kp.redshift) p[2] *= (double)sr.zf;
     if (kp.collision == COLL_FLUID) {
-        set_to_fluid<R, MED, DIMS>(kp, su, x, p);
+        set_to_fluid<R, MED, DIMS>(kp, sr, x, p);
     } else {
-        R T = jmax0(L.T);
+        const R T = jmax0(L.T);
+        const Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_MOM);
+        R uc = u.u[0];
         if (kp.collision != COLL_RTA) {
-            R xi[3];
-            momentum_noise<R, PDIM>(kp, i, s, pid, xi);
+            R xi[3], z3;
+            box_muller(u.u[0], u.u[1], xi[0], xi[1]);
+            if (PDIM == 3) {
+                box_muller(u.u[2], u.u[3], xi[2], z3);
+                if (kp.collision == COLL_LANGEVIN_RTA) uc = normcdf(z3);
+            } else {
+                xi[2] = R(0);
+                uc = u.u[2];
+            }
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) rec_slot<REC>(kp, s, i, d, xi[d]);
             langevin_kick<R, DIMS, PDIM>(kp, T, p, xi);
         }
-        if (kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA)
-            rta_collide<R, DIMS, PDIM>(kp, i, s, pid, T, p);
-        boost<R, DIMS, PDIM>(kp, L, p, true);
+        if (kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA) {
+            rec_slot<REC>(kp, s, i, 3, uc);
+            rta_collide<REC, R, DIMS, PDIM>(kp, i, s, pid, T, uc, p);
+        }
+        if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true);
     }
-    stream_positions<R, MED, DIMS, PDIM>(kp, su, i, s, pid, x, xl, p);
+    stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, pid, x, xl, p);
 }
 
-// Freeze-out latch after streaming (kernels_gpu.jl:588-635).
-template <typename R, int MED, int DIMS, int PDIM>
-__device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepU<R>& su, int64_t i,
-                                                const R (&x)[3], const R (&p)[3],
-                                                R& flag, R (&lpos)[3], R (&lmom)[3], R& ltau, R& lT)
+// Temperature at the particle in FP64 arithmetic (FP64 weights over the stored
+// field values), for the freeze-out latch of the FP32 path.
+template <typename R, int MED, int DIMS>
+__device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
+                                                   const float (&xl)[3])
 {
-    if (flag != R(0)) return;
-    R r;
-    if (DIMS == 1) r = fabs(x[0]);
-    else { R r2 = R(0);
+    const MediumDev<R>& md = kp.med;
+    double xd[3];
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
-        r = sqrt(r2); }
-    R T = temperature_at<R, MED, DIMS>(kp, su, x, r);
-    R tau = su.tR;
-    if (sizeof(R) == 4) tau = (R)su.t;
-    if (T < kp.Tfo) {
-        R frac = (kp.fo_interp && lT > kp.Tfo && lT > T) ? (lT - kp.Tfo) / (lT - T) : R(1);
+    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (double)xl[d];
+    double T;
+    if (MED == MED_BJORKEN) {
+        T = sr.Td;
+    } else if (MED == MED_RT) {
+        double r;
+        if (DIMS == 1) r = fabs(xd[0]);
+        else { double r2 = 0.0;
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos[d] + frac * (x[d] - lpos[d]);
+            for (int d = 0; d < DIMS; ++d) r2 += xd[d] * xd[d];
+            r = sqrt(r2); }
+        const double* g = md.xgd;
+        const int nr = md.nr;
+        double rq = r > g[nr - 1] ? g[nr - 1] : (r < g[0] ? g[0] : r);
+        int i = cell_index(g, nr, rq, md.x_uniform, (double)md.xg0, (double)md.xinvd);
+        double x0 = g[i], x1 = g[i + 1], dx = x1 - x0;
+        double w = fabs(dx) < kEps ? 0.0 : (rq - x0) / dx;
+        const int j = sr.kt;
+        double v00 = (double)md.TV[i + nr * j].x, v10 = (double)md.TV[i + 1 + nr * j].x;
+        double v01 = (double)md.TV[i + nr * (j + 1)].x, v11 = (double)md.TV[i + 1 + nr * (j + 1)].x;
+        double c0 = v00 * (1.0 - w) + v10 * w, c1 = v01 * (1.0 - w) + v11 * w;
+        T = c0 * (1.0 - sr.wtd) + c1 * sr.wtd;
+    } else {
+        int ix, iy;
+        double wx, wy;
+        {
+            double xq = xd[0] > md.gxl_d ? md.gxl_d : (xd[0] < md.gx0_d ? md.gx0_d : xd[0]);
+            double yq = xd[1] > md.gyl_d ? md.gyl_d : (xd[1] < md.gy0_d ? md.gy0_d : xd[1]);
+            double fx = (xq - md.gx0_d) / md.gdx_d, fy = (yq - md.gy0_d) / md.gdy_d;
+            double flx = floor(fx), fly = floor(fy);
+            ix = flx < 0.0 ? 0 : (flx > (double)(md.gnx - 2) ? md.gnx - 2 : (int)flx);
+            iy = fly < 0.0 ? 0 : (fly > (double)(md.gny - 2) ? md.gny - 2 : (int)fly);
+            wx = fx - (double)ix;
+            wy = fy - (double)iy;
+        }
+        const float4* s0 = md.G + ((size_t)sr.kt * md.gny + iy) * md.gnx + ix;
+        const float4* s1 = s0 + (size_t)md.gny * md.gnx;
+        double c[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float4* q = k ? s1 : s0;
+            double a00 = __ldg(q).x, a10 = __ldg(q + 1).x, a01 = __ldg(q + md.gnx).x, a11 = __ldg(q + md.gnx + 1).x;
+            double c0 = a00 * (1.0 - wx) + a10 * wx, c1 = a01 * (1.0 - wx) + a11 * wx;
+            c[k] = c0 * (1.0 - wy) + c1 * wy;
+        }
+        T = c[0] * (1.0 - sr.wtd) + c[1] * sr.wtd;
+    }
+    if (md.T_scale != R(1)) T *= (double)md.T_scale;
+    return T;
+}
+
+// Freeze-out latch after streaming (kernels_gpu.jl:588-635), evaluated in FP64.
+template <typename R, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
+                                                const R (&x)[3], const float (&xl)[3], const double (&p)[3],
+                                                double& flag, double (&lpos)[3], double (&lmom)[3],
+                                                double& ltau, double& lT)
+{
+    if (flag != 0.0) return;
+    double T;
+    if (sizeof(R) == 8) {
+        R r;
+        if (DIMS == 1) r = fabs(x[0]);
+        else { R r2 = R(0);
+#pragma unroll
+            for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
+            r = sqrt(r2); }
+        T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
+    } else {
+        T = temperature_fp64<R, MED, DIMS>(kp, sr, x, xl);
+    }
+    double xd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (sizeof(R) == 4 ? (double)xl[d] : 0.0);
+    const double Tfo = (double)kp.Tfo;
+    if (T < Tfo) {
+        double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos[d] + frac * (xd[d] - lpos[d]);
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom[d] + frac * (p[d] - lmom[d]);
-        kp.fo_tau[i] = (R)((double)ltau + (double)frac * (su.t - (double)ltau));
-        kp.fo_flag[i] = R(1);
-        flag = R(1);
+        kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
+        kp.fo_flag[i] = 1.0;
+        flag = 1.0;
     } else {
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) lpos[d] = x[d];
+        for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
-        ltau = (R)su.t;
+        ltau = sr.t;
         lT = T;
     }
 }
@@ -553,35 +697,15 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
 // interpolation neither clamps the query nor guards dx (kernels_cpu_GC.jl:37-57).
 // ---------------------------------------------------------------------------
 template <typename R>
-struct StepMilne { double t; int kt; R wt; };
-
-template <typename R>
-__device__ __forceinline__ StepMilne<R> milne_uniforms(const KParams<R>& kp, int64_t s)
-{
-    StepMilne<R> u;
-    u.t = __dadd_rn(__dmul_rn((double)s, kp.dt), kp.t0);
-    const double* tg = kp.med.tgd;
-    const int nt = kp.med.nt;
-    int lo = -1, hi = nt;
-    while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (__ldg(tg + mid) <= u.t) lo = mid; else hi = mid; }
-    int k = lo < 0 ? 0 : lo;
-    k = k > nt - 2 ? nt - 2 : k;
-    double y0 = __ldg(tg + k), y1 = __ldg(tg + k + 1);
-    u.kt = k;
-    u.wt = (R)((u.t - y0) / (y1 - y0));
-    return u;
-}
-
-template <typename R>
-__device__ __forceinline__ void milne_lookup(const MediumDev<R>& md, const StepMilne<R>& su, R r, R& T, R& V)
+__device__ __forceinline__ void milne_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R r, R& T, R& V)
 {
     int i = cell_index(md.xg, md.nr, r, md.x_uniform, md.xg0, md.xinvd);
     R x0 = __ldg(md.xg + i), x1 = __ldg(md.xg + i + 1);
     R xd = (r - x0) / (x1 - x0);
-    const int nr = md.nr, j = su.kt;
+    const int nr = md.nr, j = sr.kt;
     auto a00 = md.TV[i + nr * j],       a10 = md.TV[i + 1 + nr * j];
     auto a01 = md.TV[i + nr * (j + 1)], a11 = md.TV[i + 1 + nr * (j + 1)];
-    R yd = su.wt;
+    R yd = sr.wt;
     R c0 = a00.x * (R(1) - xd) + a10.x * xd;
     R c1 = a01.x * (R(1) - xd) + a11.x * xd;
     T = c0 * (R(1) - yd) + c1 * yd;
@@ -590,17 +714,19 @@ __device__ __forceinline__ void milne_lookup(const MediumDev<R>& md, const StepM
     V = c0 * (R(1) - yd) + c1 * yd;
 }
 
-template <typename R>
-__device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepMilne<R>& su, int64_t i, int64_t s,
-                                           uint32_t pid, R (&x)[3], float (&xl)[3], R (&p)[3])
+template <bool REC, typename R>
+__device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
+                                           uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
-    const R m = kp.m, dt = kp.dtR;
-    R T, v;
-    milne_lookup(kp.med, su, fabs(x[1]), T, v);       // same (r, t) for rest boost, forces, lab boost
+    const double m = (double)kp.m;
+    const R dt = kp.dtR;
+    R T, vR;
+    milne_lookup(kp.med, sr, fabs(x[1]), T, vR);      // same (r, t) for rest boost, forces, lab boost
     if (kp.med.T_scale != R(1)) T *= kp.med.T_scale;
+    const double v = (double)vR;
     // kernels_cpu_GC.jl:64-82
-    R g = R(1) / sqrt(R(1) - v * v + R(1e-10));
-    R pt = p[0], pr = p[1];
+    double g = 1.0 / sqrt(1.0 - v * v + 1e-10);
+    double pt = p[0], pr = p[1];
     p[0] = g * (pt - v * pr);
     p[1] = g * (pr - v * pt);
     // kernels_cpu_GC.jl:110-174 (Christoffel term identically zero) + :244-256
@@ -608,33 +734,46 @@ __device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepMilne
     R tn = DsT_safe == R(0) ? R(0) : eval_spline(T, kp.drag_Tmin, kp.drag_invdT, kp.drag, kp.n_drag);
     const bool ok = tn > R(0) && isfinite(tn);
     R etaD = ok ? R(1) / tn : R(0);
-    R kappa = ok ? (R(2) * m * T) / tn : R(0);
+    R kappa = ok ? (R(2) * kp.m * T) / tn : R(0);
     R kT = sqrt(kappa);
     Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_MOM);
     R xi, z1;
     box_muller(u.u[0], u.u[1], xi, z1);
-    rec_slot(kp, s, i, 0, xi);
-    R det, sto;
-    if (etaD > R(0) && dt > R(0)) {
-        R a = exp(-etaD * dt);
-        R np = kT * sqrt((R(1) - a * a) / (R(2) * etaD * dt));
-        det = (a - R(1)) * p[1];
-        sto = np * xi;
+    rec_slot<REC>(kp, s, i, 0, xi);
+    if (sizeof(R) == 8) {
+        R det, sto;
+        if (etaD > R(0) && dt > R(0)) {
+            R a = exp(-etaD * dt);
+            R np = kT * sqrt((R(1) - a * a) / (R(2) * etaD * dt));
+            det = (a - R(1)) * (R)p[1];
+            sto = np * xi;
+        } else {
+            det = R(0);
+            sto = kT * xi;
+        }
+        p[1] += (double)(det + kp.sqrt_dt * sto);
+    } else if (etaD > R(0) && dt > R(0)) {
+        R em1 = expm1_neg(etaD * dt);
+        R amp = sqrt(m * T * (-em1 * (R(2) + em1)));     // sqrt(kappa (1-a^2) / (2 eta_D))
+        p[1] += (double)(em1 * (R)p[1] + amp * xi);
     } else {
-        det = R(0);
-        sto = kT * xi;
+        p[1] += (double)(kp.sqrt_dt * (kT * xi));
     }
-    p[1] += det + kp.sqrt_dt * sto;
     p[0] = sqrt(m * m + p[1] * p[1]);
     // kernels_cpu_GC.jl:85-102
-    g = R(1) / sqrt(R(1) - v * v + R(1e-8));
+    g = 1.0 / sqrt(1.0 - v * v + 1e-8);
     pt = p[0]; pr = p[1];
     p[0] = g * (pt + v * pr);
     p[1] = g * (pr + v * pt);
     // kernels_cpu_GC.jl:259-274
-    R E = p[0];
-    acc_add(x[0], xl[0], sizeof(R) == 8 ? dt * p[0] / E : dt);
-    acc_add(x[1], xl[1], dt * p[1] / E);
+    if (sizeof(R) == 8) {
+        double E = p[0];
+        acc_add(x[0], xl[0], (R)(dt * p[0] / E));
+        acc_add(x[1], xl[1], (R)(dt * p[1] / E));
+    } else {
+        acc_add(x[0], xl[0], dt);
+        acc_add(x[1], xl[1], (R)((double)dt * p[1] / p[0]));
+    }
 }
 
 }  // namespace lim

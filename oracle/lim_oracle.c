@@ -251,39 +251,57 @@ static inline void box_muller(double u0, double u1, double* z0, double* z1)
 
 /* Per-step variates of one particle, slot layout shared with the engine:
  *   0..2 momentum normals, 3 u_collide, 4 u_sample, 5..7 RTA direction
- *   normals, 8..10 position-diffusion normals. */
+ *   normals, 8..10 position-diffusion normals.
+ * Group MOM: (u0,u1) -> (xi0, xi1), (u2,u3) -> (xi2, z3).  The collision uniform is
+ * Phi(z3) when pdim = 3 (z3 is independent of xi0..xi2), u2 when pdim < 3, and u0
+ * when there is no Langevin kick.  Group RTA (only when a particle collides):
+ * u_sample = u0, (u1,u2) -> (g0, g1); group RTADIR: (u0,u1) -> g2. */
 typedef struct noise_src {
     const double* rec;      /* recorded buffer or NULL (Philox) */
     int64_t rec_first, rec_steps, n;
 } noise_src;
 
-static void draw_momentum(const orc_params* P, const noise_src* ns, int64_t i, int64_t step, double xi[3])
+static inline double rec_at(const noise_src* ns, int64_t i, int64_t step, int slot)
+{
+    return ns->rec[((step - ns->rec_first) * ORC_NOISE_SLOTS + slot) * ns->n + i];
+}
+
+static void draw_step(const orc_params* P, const noise_src* ns, int64_t i, int64_t step, int kick, double xi[3],
+                      double* uc)
 {
     if (ns->rec) {
-        const double* b = ns->rec + ((step - ns->rec_first) * ORC_NOISE_SLOTS) * ns->n + i;
-        for (int k = 0; k < 3; ++k) xi[k] = b[k * ns->n];
+        for (int k = 0; k < 3; ++k) xi[k] = rec_at(ns, i, step, k);
+        *uc = rec_at(ns, i, step, 3);
         return;
     }
-    double u[4], z3;
+    double u[4], z3 = 0.0;
     uniforms4(P, P->particle_offset + i, step, TAG_MOM, u);
+    if (!kick) { xi[0] = xi[1] = xi[2] = 0.0; *uc = u[0]; return; }
     box_muller(u[0], u[1], &xi[0], &xi[1]);
-    box_muller(u[2], u[3], &xi[2], &z3);
+    if (P->pdim == 3) {
+        box_muller(u[2], u[3], &xi[2], &z3);
+        *uc = 0.5 * erfc(-z3 * 0.70710678118654752440);
+    } else {
+        xi[2] = 0.0;
+        *uc = u[2];
+    }
 }
-static void draw_rta_uniforms(const orc_params* P, const noise_src* ns, int64_t i, int64_t step,
-                              double* uc, double* us, double g[3])
+static void draw_rta_sample(const orc_params* P, const noise_src* ns, int64_t i, int64_t step, double* us, double g[3])
 {
     if (ns->rec) {
-        const double* b = ns->rec + ((step - ns->rec_first) * ORC_NOISE_SLOTS) * ns->n + i;
-        *uc = b[3 * ns->n]; *us = b[4 * ns->n];
-        for (int k = 0; k < 3; ++k) g[k] = b[(5 + k) * ns->n];
+        *us = rec_at(ns, i, step, 4);
+        for (int k = 0; k < 3; ++k) g[k] = rec_at(ns, i, step, 5 + k);
         return;
     }
     double u[4], v[4], z;
     uniforms4(P, P->particle_offset + i, step, TAG_RTA, u);
-    *uc = u[0]; *us = u[1];
-    box_muller(u[2], u[3], &g[0], &g[1]);
-    uniforms4(P, P->particle_offset + i, step, TAG_RTADIR, v);
-    box_muller(v[0], v[1], &g[2], &z);
+    *us = u[0];
+    box_muller(u[1], u[2], &g[0], &g[1]);
+    g[2] = 0.0;
+    if (P->pdim == 3) {
+        uniforms4(P, P->particle_offset + i, step, TAG_RTADIR, v);
+        box_muller(v[0], v[1], &g[2], &z);
+    }
 }
 static void draw_diffusion(const orc_params* P, const noise_src* ns, int64_t i, int64_t step, double d[3])
 {
@@ -503,12 +521,15 @@ static void langevin_kick(const orc_params* P, const orc_medium* md, double* p, 
 
 /* kernels_gpu.jl:653-704 with injected uniforms (the CPU twin kernels_cpu.jl:474-508
  * draws from the global RNG and cannot be fed identical noise). */
-static void rta_collide(const orc_params* P, const orc_medium* md, double* p, double T,
-                        double uc, double us, const double g[3])
+static void rta_collide(const orc_params* P, const orc_medium* md, const noise_src* ns, int64_t i, int64_t step,
+                        double* p, double T, double uc)
 {
     double tn = (P->DsT > 0.0 && T > 0.0) ? eval_spline(T, md->rta_Tmin, md->rta_invdT, md->rta, md->n_rta) : 0.0;
     double Pcol = (tn > 0.0 && jl_isfinite(tn)) ? jl_clamp(P->dt / tn, 0.0, 1.0) : 1.0;
-    if (!(uc < Pcol)) return;
+    /* rand() < Pcol with rand() in [0,1): Pcol = 1 always collides */
+    if (!(uc < Pcol || Pcol >= 1.0)) return;
+    double us, g[3];
+    draw_rta_sample(P, ns, i, step, &us, g);
     double pstar = invcdf_lookup(md, us, T);
     if (P->dims == 1) { p[0] = (g[0] < 0.0 ? -1.0 : 1.0) * pstar; return; }
     double nrm2 = 0.0;
@@ -662,16 +683,11 @@ static void cart_step(const orc_params* P, const orc_medium* md, const noise_src
         for (int64_t d = 0; d < P->dims; ++d) r2 += x[d] * x[d];
         double r = sqrt(r2);
         double T = jl_max(medium_T(md, x, r, t), 0.0);
-        if (P->collision == C_LANGEVIN || P->collision == C_LANGEVIN_RTA) {
-            double xi[3];
-            draw_momentum(P, ns, i, step, xi);
-            langevin_kick(P, md, p, T, xi);
-        }
-        if (P->collision == C_RTA || P->collision == C_LANGEVIN_RTA) {
-            double uc, us, g[3];
-            draw_rta_uniforms(P, ns, i, step, &uc, &us, g);
-            rta_collide(P, md, p, T, uc, us, g);
-        }
+        const int kick = P->collision == C_LANGEVIN || P->collision == C_LANGEVIN_RTA;
+        double xi[3], uc;
+        draw_step(P, ns, i, step, kick, xi, &uc);
+        if (kick) langevin_kick(P, md, p, T, xi);
+        if (P->collision == C_RTA || P->collision == C_LANGEVIN_RTA) rta_collide(P, md, ns, i, step, p, T, uc);
         do_boost(P, &f, p, 1);
     }
     update_positions(P, md, ns, i, step, x, p, t);
@@ -704,8 +720,8 @@ static void milne_step(const orc_params* P, const orc_medium* md, const noise_sr
     for (int nu = 0; nu < 2; ++nu)
         for (int rho = 0; rho < 2; ++rho) geo += -0.0 * p[nu] * p[rho] / p0;
     geo *= dt;
-    double xi[3];
-    draw_momentum(P, ns, i, step, xi);
+    double xi[3], uc_unused;
+    draw_step(P, ns, i, step, 1, xi, &uc_unused);
     double det, sto;
     if (etaD > 0.0 && dt > 0.0) {
         double a = exp(-etaD * dt);
@@ -798,6 +814,19 @@ double orc_eval_spline(double T, double Tmin, double invdT, const double* vals, 
 double orc_invcdf_lookup(const orc_medium* md, double u, double T) { return invcdf_lookup(md, u, T); }
 void orc_uniforms4(const orc_params* P, int64_t pid, int64_t step, int tag, double u[4])
 { uniforms4(P, pid, step, tag, u); }
+/* The variates the engine draws for (particle i, step) in recording-slot order,
+ * as if the particle collided (slots 4..7 are drawn regardless). */
+void orc_step_variates(const orc_params* P, int64_t i, int64_t step, int kick, double out[11])
+{
+    noise_src ns = { NULL, 0, 0, 0 };
+    double xi[3], uc, us, g[3], d[3];
+    for (int k = 0; k < 11; ++k) out[k] = 0.0;
+    draw_step(P, &ns, i, step, kick, xi, &uc);
+    draw_rta_sample(P, &ns, i, step, &us, g);
+    draw_diffusion(P, &ns, i, step, d);
+    for (int k = 0; k < 3; ++k) { out[k] = xi[k]; out[5 + k] = g[k]; out[8 + k] = d[k]; }
+    out[3] = uc; out[4] = us;
+}
 int64_t orc_sizeof_params(void) { return (int64_t)sizeof(orc_params); }
 int64_t orc_sizeof_medium(void) { return (int64_t)sizeof(orc_medium); }
 int64_t orc_sizeof_fo(void) { return (int64_t)sizeof(fo_state); }

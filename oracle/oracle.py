@@ -81,6 +81,8 @@ def lib() -> C.CDLL:
         for f in ("orc_sizeof_params", "orc_sizeof_medium", "orc_sizeof_fo"):
             getattr(L, f).restype = C.c_int64
         L.orc_max_threads.restype = C.c_int
+        L.orc_step_variates.argtypes = [C.POINTER(OrcParams), C.c_int64, C.c_int64, C.c_int, _DP]
+        L.orc_step_variates.restype = None
         assert L.orc_sizeof_params() == C.sizeof(OrcParams)
         assert L.orc_sizeof_medium() == C.sizeof(OrcMedium)
         assert L.orc_sizeof_fo() == FO_FIELDS * 8
@@ -225,6 +227,13 @@ def uniforms4(P, pid, step, tag):
     u = np.zeros(4)
     lib().orc_uniforms4(C.byref(P), pid, step, tag, _d(u))
     return u
+
+
+def step_variates(P, pid, step, kick=True):
+    """The 11 recording slots the engine draws for (particle, step), as if it collided."""
+    out = np.zeros(NOISE_SLOTS)
+    lib().orc_step_variates(C.byref(P), pid, step, int(bool(kick)), _d(out))
+    return out
 
 
 def max_threads() -> int:

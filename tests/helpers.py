@@ -107,9 +107,38 @@ def oracle_drive(orc, *, xgrid, tgrid, Tf, Vf, x0, p0, M, DsT, dt, t0, tfinal, s
     return times, mh, xh, out
 
 
-def parity(a, b, scale):
-    """Per-component |a-b| / max(|b|, 1e-3 scale): returns (max, p99)."""
+def parity(a, b, scale, floor=1e-3):
+    """Per-particle relative error ||a_i - b_i|| / max(||b_i||, floor * scale) over the
+    rows of (rows, N) arrays; returns (max, p99).  scale: 0.3 GeV for momenta, 1 fm
+    for positions."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    e = np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * scale)
-    return float(np.max(e)) if e.size else 0.0, float(np.percentile(e, 99)) if e.size else 0.0
+    if a.ndim == 1:
+        a, b = a[None, :], b[None, :]
+    if a.size == 0:
+        return 0.0, 0.0
+    e = np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), floor * scale)
+    return float(np.max(e)), float(np.percentile(e, 99))
+
+
+def oracle_medium(orc, wl):
+    """The restatement's medium/tables from a workload description."""
+    med = wl.medium
+    md = orc.Medium()
+    if med["kind"] == "rt":
+        md.rt(med["xgrid"], med["tgrid"], med["T"], med["V"], med.get("V2"))
+    elif med["kind"] == "bjorken":
+        md.bjorken(med["T0"], med["tau0"], med["power"], med["r_max"])
+    else:
+        md.grid(med["T"], med["ux"], med["uy"], med["x0"], med["dx"], med["y0"], med["dy"], med["tau0"], med["dtau"])
+    for w, (a, b, v) in wl.splines.items():
+        md.spline(w, a, b, v)
+    if wl.invcdf is not None:
+        md.invcdf(*wl.invcdf)
+    return md
+
+
+def oracle_params(orc, wl, **over):
+    d = dict(wl.params)
+    d.update(over)
+    return orc.make_params(**d)

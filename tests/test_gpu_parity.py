@@ -1,0 +1,247 @@
+"""Per-particle parity of the CUDA engine (through the C-ABI) against the CPU FP64
+restatement on identical counter-based noise.
+
+Metric: per particle ||a - b|| / max(||b||, floor * s), s = 0.3 GeV for momenta and
+1 fm for positions, max over particles.
+  FP64 gate 1e-12 with floor 1e-3 (relative down to 0.3 MeV / 1e-3 fm).
+  FP32 gate 1e-5 with floor 1: FP32 arithmetic errs by ~eps * E in absolute terms,
+  so it is gated at the natural momentum and length scales; the strict (floor
+  1e-3) figure is printed beside it.
+RTA accept/reject decisions must be identical: a flipped decision moves a momentum
+by O(1) and fails either gate."""
+import numpy as np
+import pytest
+
+from helpers import oracle_medium, oracle_params, parity
+from parity_cases import CASES, build_case
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp32": 1e-5}
+
+
+def engine_run(lmb, wl, *, record=False, save_every=0, nslots=0, split=None):
+    eng = lmb.capi.Engine(0)
+    lmb.workloads.configure(eng, wl)
+    cart = wl.params.get("coords", 0) == 0
+    if cart:
+        eng.initial_lab_boost()
+    x0, p0 = eng.download_state()
+    if record:
+        eng.record_noise(wl.first_step, wl.steps)
+    hx = hp = None
+    if save_every:
+        hx = np.zeros(nslots * wl.n * int(eng.params.dims))
+        hp = np.zeros(nslots * wl.n * int(eng.params.pdim))
+    if split:
+        eng.run(wl.first_step, split, save_every, 0, hx, hp)
+        eng.run(wl.first_step + split, wl.steps - split, save_every, 0, hx, hp)
+    else:
+        eng.run(wl.first_step, wl.steps, save_every, 0, hx, hp)
+    x, p = eng.download_state()
+    out = dict(x0=x0, p0=p0, x=x, p=p, hx=hx, hp=hp)
+    if wl.params.get("freezeout_capture"):
+        out["fo"] = eng.download_freezeout()
+    if record:
+        out["rec"] = eng.download_noise()
+    out["obs"] = eng.observables()
+    eng.close()
+    return out
+
+
+def oracle_run(orc, wl, x0, p0, *, rec=None, save_every=0, nslots=0, **over):
+    P = oracle_params(orc, wl, **over)
+    md = oracle_medium(orc, wl)
+    return orc.run(P, md, x0, p0, wl.first_step, wl.steps, save_every=save_every, nslots=nslots, rec=rec)
+
+
+def assert_parity(tag, g, o, tol, T=0.3, floor=1e-3, mask=None):
+    gx, ox, gp, op = g["x"], o["x"], g["p"], o["p"]
+    if mask is not None:
+        gx, ox, gp, op = gx[:, mask], ox[:, mask], gp[:, mask], op[:, mask]
+    ex = parity(gx, ox, 1.0, floor)
+    ep = parity(gp, op, T, floor)
+    sx = parity(gx, ox, 1.0, 1e-3)
+    sp = parity(gp, op, T, 1e-3)
+    print(f"{tag}: x max {ex[0]:.3g} p99 {ex[1]:.3g} | p max {ep[0]:.3g} p99 {ep[1]:.3g}"
+          f" | strict x {sx[0]:.3g} p {sp[0]:.3g}")
+    assert ex[0] <= tol and ep[0] <= tol, (tag, ex, ep)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp64_parity(lmb, orc, name):
+    wl = build_case(name, "fp64")
+    over = {"stop_after_freezeout": 0}
+    wl.params.update(over)
+    g = engine_run(lmb, wl)
+    P = oracle_params(orc, wl)
+    md = oracle_medium(orc, wl)
+    if wl.params.get("coords", 0) == 0:
+        x0, p0 = orc.initial_lab_boost(P, md, wl.x, wl.p)
+        assert parity(g["p0"], p0, 0.3)[0] <= TOL["fp64"]
+    else:
+        x0, p0 = wl.x, wl.p
+    o = orc.run(P, md, x0, p0, wl.first_step, wl.steps)
+    assert o["first_bad"] == -1
+    assert_parity(f"{name} fp64", g, o, TOL["fp64"])
+    if "fo" in g:
+        assert np.array_equal(g["fo"]["flag"], o["fo_flag"])
+        assert parity(g["fo"]["pos"], o["fo_pos"], 1.0)[0] <= TOL["fp64"]
+        assert parity(g["fo"]["mom"], o["fo_mom"], 0.3)[0] <= TOL["fp64"]
+        assert parity(g["fo"]["tau"], o["fo_tau"], 1.0)[0] <= TOL["fp64"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fp32_parity_recorded_noise(lmb, orc, name):
+    """FP32 engine vs FP64 restatement fed the variates the engine consumed."""
+    wl = build_case(name, "fp32")
+    check_fo_outputs(lmb, orc, wl, name, record=True)
+
+
+@pytest.mark.parametrize("name", ["static3d", "lrta_bjorken_table", "grid_lrta_fo", "milne"])
+def test_fp32_parity_philox(lmb, orc, name):
+    """FP32 engine vs FP64 restatement regenerating the FP32 uniforms from Philox
+    (the whole FP32 error: arithmetic plus the FP32 noise transform)."""
+    wl = build_case(name, "fp32")
+    check_fo_outputs(lmb, orc, wl, name, record=False)
+
+
+def check_fo_outputs(lmb, orc, wl, name, record):
+    """FP32 comparison with the production freeze-out semantics: a latched particle
+    stops (its outputs are the latch), so the latch arrays of particles latched in
+    both runs and the states of never-latched particles are compared."""
+    g = engine_run(lmb, wl, record=record)
+    o = oracle_run(orc, wl, g["x0"], g["p0"], rec=g.get("rec"), precision=1)
+    tag = f"{name} fp32/{'rec' if record else 'philox'}"
+    if "fo" not in g:
+        assert_parity(tag, g, o, TOL["fp32"], floor=1.0)
+        return
+    gf, of = g["fo"]["flag"], o["fo_flag"]
+    assert np.mean(gf == of) >= 0.999, np.mean(gf == of)
+    live = (gf == 0) & (of == 0)
+    both = (gf == 1) & (of == 1)
+    assert_parity(tag + " live", g, o, TOL["fp32"], floor=1.0, mask=live)
+    # The latch interpolates to T = Tfo with frac = (T_prev - Tfo)/(T_prev - T), whose
+    # condition number is T/(T_prev - T) ~ 1e2-1e3: FP32-level trajectory differences
+    # reach the latched outputs amplified by it.  Gate: 99th percentile 1e-5, max 1e-4.
+    ep = parity(g["fo"]["mom"][:, both], o["fo_mom"][:, both], 0.3, 1.0)
+    ex = parity(g["fo"]["pos"][:, both], o["fo_pos"][:, both], 1.0, 1.0)
+    et = parity(g["fo"]["tau"][both], o["fo_tau"][both], 1.0, 1.0)
+    print(f"{tag} latched: x max {ex[0]:.3g} p99 {ex[1]:.3g} | p max {ep[0]:.3g} p99 {ep[1]:.3g} | tau max {et[0]:.3g}")
+    for e in (ep, ex, et):
+        assert e[1] <= TOL["fp32"] and e[0] <= 10 * TOL["fp32"], (tag, ep, ex, et)
+
+
+def test_fp64_recorded_noise_matches_regenerated(lmb, orc):
+    """The variates the FP64 kernel consumed are the ones the restatement regenerates
+    from the same Philox counters (to libm-vs-device rounding of log/sincos/erfc)."""
+    wl = build_case("lrta_bjorken_table", "fp64", N=512, steps=40)
+    g = engine_run(lmb, wl, record=True)
+    P = oracle_params(orc, wl)
+    rec = g["rec"]
+    collided = 0
+    for s in range(wl.steps):
+        for i in range(0, 512, 7):
+            v = orc.step_variates(P, i, wl.first_step + s)
+            assert np.allclose(rec[s, 0:4, i], v[0:4], rtol=1e-14, atol=1e-15)
+            if rec[s, 4, i] != 0.0:               # recorded only when the particle collided
+                collided += 1
+                assert rec[s, 4, i] == v[4]       # raw uniform: bit-identical
+                assert np.allclose(rec[s, 5:8, i], v[5:8], rtol=1e-14, atol=1e-15)
+    assert collided > 0
+    o = oracle_run(orc, wl, g["x0"], g["p0"], rec=rec)
+    assert_parity("fp64/rec", g, o, 1e-13)
+
+
+def test_history_snapshots(lmb, orc):
+    wl = build_case("flow2d", "fp64", N=1024, steps=100)
+    g = engine_run(lmb, wl, save_every=25, nslots=5)
+    P = oracle_params(orc, wl)
+    md = oracle_medium(orc, wl)
+    x0, p0 = orc.initial_lab_boost(P, md, wl.x, wl.p)
+    o = orc.run(P, md, x0, p0, 1, 100, save_every=25, nslots=5)
+    n = wl.n
+    for k in range(1, 5):
+        gx = g["hx"][k * n * 2:(k + 1) * n * 2].reshape(n, 2).T
+        gp = g["hp"][k * n * 2:(k + 1) * n * 2].reshape(n, 2).T
+        assert parity(gx, o["hist_x"][k], 1.0)[0] <= 1e-12
+        assert parity(gp, o["hist_p"][k], 0.3)[0] <= 1e-12
+
+
+def test_chunked_run_is_bit_identical(lmb):
+    """Counter-based noise: splitting the step range across launches changes nothing."""
+    for prec in ("fp64", "fp32"):
+        wl = build_case("lrta_bjorken_table", prec, N=4096, steps=120)
+        a = engine_run(lmb, wl)
+        b = engine_run(lmb, wl, split=47)
+        assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["p"], b["p"])
+
+
+def test_philox_device_matches_host(lmb, orc):
+    eng = lmb.capi.Engine(0)
+    rng = np.random.default_rng(5)
+    for _ in range(64):
+        ctr = [int(v) for v in rng.integers(0, 2 ** 32, 4, dtype=np.uint64)]
+        key = [int(v) for v in rng.integers(0, 2 ** 32, 2, dtype=np.uint64)]
+        assert eng.philox(ctr, key) == orc.philox(ctr, key)
+    eng.close()
+
+
+def test_empty_ensemble(lmb):
+    wl = build_case("flow2d", "fp64", N=4, steps=10)
+    wl.x = wl.x[:, :0]
+    wl.p = wl.p[:, :0]
+    eng = lmb.capi.Engine(0)
+    lmb.workloads.configure(eng, wl)
+    eng.initial_lab_boost()
+    eng.run(1, 10)
+    x, p = eng.download_state()
+    assert x.shape == (2, 0) and p.shape == (2, 0)
+    assert eng.observables()["count"] == 0
+    eng.close()
+
+
+def test_nonfinite_state_is_reported(lmb):
+    """simulate_cpu.jl:293-303: NaN/Inf in the state stops the run with the step."""
+    wl = build_case("flow2d", "fp64", N=256, steps=10)
+    wl.p[0, 100] = np.nan
+    eng = lmb.capi.Engine(0)
+    lmb.workloads.configure(eng, wl)
+    with pytest.raises(lmb.capi.LimError, match="NaN/Inf at step 1") as ei:
+        eng.run(1, 10)
+    assert ei.value.code == lmb.capi.LIM_ERR_NONFINITE
+    assert eng.status() == 1
+    eng.close()
+
+
+def test_parameter_validation(lmb):
+    capi = lmb.capi
+    eng = capi.Engine(0)
+    with pytest.raises(capi.LimError, match="momentum_dimensions=4 with dimensions=2"):
+        eng.set_params(dims=2, pdim=4)
+    with pytest.raises(capi.LimError, match="bjorken_redshift requires dimensions=2"):
+        eng.set_params(dims=3, pdim=3, bjorken_redshift=1, t0=1.0)
+    with pytest.raises(capi.LimError, match="initial_time > 0"):
+        eng.set_params(dims=2, pdim=3, bjorken_redshift=1, t0=0.0)
+    with pytest.raises(capi.LimError, match="collision_mode"):
+        eng.set_params(collision=9)
+    with pytest.raises(capi.LimError) as ei:
+        eng.set_medium_rt([0.0, 0.0, 1.0], [0.0, 1.0], np.zeros((3, 2)), np.zeros((3, 2)))
+    assert ei.value.code == capi.LIM_ERR_ARG
+    eng.set_params(dims=2, pdim=2)
+    with pytest.raises(capi.LimError, match="no medium"):
+        eng.run(1, 1)
+    eng.close()
+
+
+def test_observables_match_host_reduction(lmb):
+    wl = build_case("lrta_bjorken_table", "fp64", N=20000, steps=50)
+    g = engine_run(lmb, wl)
+    p = g["p"]
+    pt = np.hypot(p[0], p[1])
+    obs = g["obs"]
+    assert obs["count"] == wl.n
+    assert np.isclose(obs["mean_pt"], pt.mean(), rtol=1e-12)
+    assert np.isclose(obs["mean_cos2phi"], np.mean((p[0] ** 2 - p[1] ** 2) / pt ** 2), rtol=1e-10)
+    assert np.isclose(obs["frac_pt_gt"], np.mean(pt > 5.0), rtol=1e-12)
+    assert np.isclose(obs["mean_p2"], np.mean(np.sum(p ** 2, axis=0)), rtol=1e-12)
