@@ -199,6 +199,22 @@ int lim_download_freezeout(lim_ctx* ctx, double* fo_pos, double* fo_mom,
  * from_freezeout != 0): out[LIM_OBS_NUM] (see the LIM_OBS_* enumeration). */
 int lim_observables(lim_ctx* ctx, int from_freezeout, double* out);
 
+/* Observables of a caller-owned device ensemble without allocating anything.
+ * No counterpart in the reference: it serves hosts that cannot call cudaMalloc
+ * (memory comes from their own pool, e.g. CUDA.jl's, or the call runs where
+ * allocation is not allowed).  p_dev: (pdim, n) column-major doubles on `device`;
+ * x_dev: (dims, n) or NULL; out_dev: LIM_OBS_NUM doubles on the device receiving
+ * the SUMS (out[LIM_OBS_COUNT] = n; divide for means).  Enqueued on `stream`
+ * (NULL = default stream); read out_dev after the stream reaches the call.
+ * Limits and sharing: n <= 16,777,216; the per-block partial sums live in one
+ * fixed 96 KiB device array of the library, held by every GPU that loads it until
+ * the process exits, shared by all calls: calls that overlap on the GPU (e.g. on
+ * two streams at once) race.  The first call on a device looks up that array's
+ * device address; make it before any stream capture.  Errors: lim_last_error(NULL). */
+int lim_observables_noalloc(int device, const double* p_dev, int64_t pdim, const double* x_dev,
+                            int64_t dims, int64_t n, double m, double pt_cut, double pt_width,
+                            double* out_dev, void* stream);
+
 /* Debug/parity mode: record every random variate the kernel consumes into a
  * device buffer of nsteps * LIM_NOISE_SLOTS * n doubles, laid out
  * [step - first_step][slot][particle]; lim_download_noise copies it out.

@@ -81,6 +81,8 @@ _SIGS = {
     "lim_philox_device": ([C.c_void_p, _U32P, _U32P, _U32P], C.c_int),
     "lim_last_run_stats": ([C.c_void_p, _DP, _I64P], C.c_int),
     "lim_probe_fma_rate": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_observables_noalloc": ([C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_double,
+                                 C.c_double, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 

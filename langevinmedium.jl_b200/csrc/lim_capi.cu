@@ -496,6 +496,8 @@ int observables_impl(lim_ctx* c, int from_fo, double* out)
 
 }  // namespace
 
+void lim::set_noctx_error(const char* msg) { g_create_error = msg; }
+
 // ===========================================================================
 // C-ABI
 // ===========================================================================
