@@ -232,6 +232,47 @@ int lim_philox_device(lim_ctx* ctx, const uint32_t ctr[4], const uint32_t key[2]
  * context stream) and the number of kernel launches it issued. */
 int lim_last_run_stats(lim_ctx* ctx, double* kernel_ms, int64_t* launches);
 
+/* ---- batches ------------------------------------------------------------------
+ * Many independent ensembles — each a configured context with its own particle
+ * count, step range, mass, transport tables and medium — advanced together: every
+ * chunk of steps is one persistent launch over all ensembles' particle tiles, and the
+ * chunk sequence is captured once as a CUDA graph and replayed.  No counterpart in
+ * the reference (one ensemble per simulate_ensemble_bulk call); a batch gives the
+ * same per-particle results as running each context with lim_run (same noise: a
+ * particle's variates depend on (seed, particle_offset + index, step) only).
+ *
+ * Every ensemble of a batch shares the precision, dims/pdim, the seed, Cartesian
+ * coordinates and the freeze-out switch; noise recording is ignored.  Contexts are
+ * referenced, not copied: they must outlive the batch, and their state is advanced
+ * in place (read it with lim_download_state).  A change to a context (parameters,
+ * medium, tables, a new upload) is picked up by the next lim_batch_run. */
+typedef struct lim_batch lim_batch;
+
+typedef struct lim_batch_shape {
+    int64_t block;          /* threads (particles) per block: 64, 128 or 256; 0 = 256 */
+    int64_t chunk_steps;    /* steps per chunk launch; 0 = the longest ensemble's range */
+    int64_t blocks_per_sm;  /* persistent blocks per SM; 0 = the occupancy maximum */
+    int64_t reg_cap;        /* FP32: 1 caps registers for four 256-thread blocks per SM */
+} lim_batch_shape;
+
+int lim_batch_create(int device, void* stream, lim_batch** out);
+int lim_batch_destroy(lim_batch* b);
+const char* lim_batch_last_error(const lim_batch* b);   /* b = NULL: the last create error */
+/* Adds `ensemble` advancing steps [first_step, first_step + nsteps); *index = its position. */
+int lim_batch_add(lim_batch* b, lim_ctx* ensemble, int64_t first_step, int64_t nsteps, int64_t* index);
+int lim_batch_set_shape(lim_batch* b, const lim_batch_shape* shape);
+int lim_batch_get_shape(const lim_batch* b, lim_batch_shape* shape);
+/* Runs every ensemble through its range: one graph replay.  LIM_ERR_NONFINITE names the
+ * first ensemble and step that produced NaN/Inf. */
+int lim_batch_run(lim_batch* b);
+/* Autotuner: times each candidate shape on the batch itself (every ensemble's state
+ * is saved first and restored before each trial and at the end) and keeps the
+ * fastest.  Candidates: block {128, 256} x chunk {64, 256, 1024, whole range} x
+ * reg_cap {0, 1} (FP32).  *best and *best_ms (may be NULL) receive the choice. */
+int lim_batch_tune(lim_batch* b, lim_batch_shape* best, double* best_ms);
+/* Device time of the last lim_batch_run (ms), its kernel launches and particle-steps. */
+int lim_batch_stats(const lim_batch* b, double* ms, int64_t* launches, int64_t* particle_steps);
+
 #ifdef __cplusplus
 }
 #endif

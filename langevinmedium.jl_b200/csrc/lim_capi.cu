@@ -14,63 +14,15 @@
 #include <vector>
 #include "../../include/langevin_b200.h"
 #include "../../include/langevin_b200_diag.h"
-#include "lim_internal.h"
+#include "lim_ctx.h"
 
 using namespace lim;
 
 namespace {
 
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
 thread_local std::string g_create_error;
 
 }  // namespace
-
-struct lim_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    std::string err;
-
-    lim_params P{};
-    bool have_params = false;
-
-    // host copy of the medium
-    int med_kind = -1;
-    std::vector<double> xg, tg, T, V, V2;
-    double bj_T0 = 0, bj_tau0 = 0, bj_power = 0, bj_rmax = 0;
-    int64_t gnx = 0, gny = 0, gnt = 0;
-    double gx0 = 0, gdx = 0, gy0 = 0, gdy = 0, gt0 = 0, gdt = 0;
-    std::vector<float> gT, gux, guy;
-    std::vector<double> spl[2];
-    double spl_Tmin[2] = { 0, 0 }, spl_invdT[2] = { 1, 1 };
-    std::vector<double> icdf;
-    int64_t nU = 0, nT = 0;
-    double ic_Tmin = 0, ic_invdT = 1;
-    double T_scale = 1.0;
-
-    // device copy of the medium for `dev_prec`
-    int dev_prec = -1;
-    bool dev_dirty = true;
-    DevBuf d_xg, d_tg, d_tgd, d_xgd, d_TV, d_V2, d_G, d_spl[2], d_icdf;
-
-    // particle state (structure of arrays, precision `state_prec`)
-    int64_t n = 0;
-    int dims = 0, pdim = 0, state_prec = -1;
-    bool have_state = false;
-    DevBuf d_x[3], d_xlo[3], d_p[3];
-    DevBuf d_fo_pos[3], d_fo_mom[3], d_fo_tau, d_fo_flag, d_l_pos[3], d_l_mom[3], d_l_tau, d_l_T;
-    DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe, d_steps;
-    DevBuf d_rec, d_ckpt;
-    int64_t rec_first = 0, rec_steps = 0, ckpt_n = -1;
-
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double last_ms = 0.0;
-    int64_t last_launches = 0;
-};
 
 namespace {
 
@@ -212,6 +164,10 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
     kp.integrator = (int)P.integrator_mode; kp.fo_capture = P.freezeout_capture != 0;
     kp.fo_interp = P.freezeout_interp != 0; kp.stop_fo = P.stop_after_freezeout != 0 && P.freezeout_capture != 0;
     kp.seed_lo = (uint32_t)(uint64_t)P.seed; kp.seed_hi = (uint32_t)((uint64_t)P.seed >> 32);
+    {
+        uint32_t k0 = kp.seed_lo, k1 = kp.seed_hi;       // Philox-4x32-10 key schedule
+        for (int r = 0; r < 10; ++r) { kp.rk[r] = make_uint2(k0, k1); k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    }
     kp.pid_offset = P.particle_offset;
     kp.n = c->n; kp.dims = c->dims; kp.pdim = c->pdim;
     kp.drag = (const R*)c->d_spl[0].p; kp.n_drag = (int)c->spl[0].size();
@@ -232,6 +188,7 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
             }
         }
     }
+    kp.spl_shared = kp.n_drag == kp.n_rta && kp.drag_Tmin == kp.rta_Tmin && kp.drag_invdT == kp.rta_invdT;
     kp.icdf = (const R*)c->d_icdf.p; kp.nU = (int)c->nU; kp.nT = (int)c->nT;
     kp.ic_Tmin = (R)c->ic_Tmin; kp.ic_invdT = (R)c->ic_invdT;
     MediumDev<R>& md = kp.med;
@@ -330,7 +287,7 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
         kp.step_base = s;
         kp.step_cap = chunk_end - s;
         LIM_CUDA(c, launch_steps<R>(kp, (int)c->P.coords, s, chunk_end, block, c->stream));
-        ++launches;
+        launches += 2;                     // the per-step table, then the fused step kernel
         const int64_t last = chunk_end - 1;
         if (saving && last % save_every == 0 && last >= 0) {
             const int64_t slot = last / save_every - first_slot;
@@ -498,6 +455,24 @@ int observables_impl(lim_ctx* c, int from_fo, double* out)
 
 void lim::set_noctx_error(const char* msg) { g_create_error = msg; }
 
+namespace lim {
+
+int ctx_fail(lim_ctx* c, int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return fail(c, code, "%s", buf);
+}
+int ctx_check_ready(lim_ctx* c) { return check_ready(c); }
+template <typename R> int ctx_build_kparams(lim_ctx* c, KParams<R>& kp) { return build_kparams<R>(c, kp); }
+template int ctx_build_kparams<double>(lim_ctx*, KParams<double>&);
+template int ctx_build_kparams<float>(lim_ctx*, KParams<float>&);
+
+}  // namespace lim
+
 // ===========================================================================
 // C-ABI
 // ===========================================================================
@@ -579,6 +554,7 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
 int lim_set_params(lim_ctx* c, const lim_params* P)
 {
     if (!c || !P) return LIM_ERR_ARG;
+    ++c->gen;
     lim_params q = *P;
     if (!std::isfinite(q.dt) || !std::isfinite(q.t0) || !std::isfinite(q.m))
         return fail(c, LIM_ERR_ARG, "dt, t0 and m must be finite");
@@ -610,12 +586,14 @@ int lim_set_params(lim_ctx* c, const lim_params* P)
     if (q.precision != LIM_FP64 && q.precision != LIM_FP32) return fail(c, LIM_ERR_ARG, "precision must be LIM_FP64 or LIM_FP32");
     if (q.block_size < 0 || q.block_size > 1024 || (q.block_size % 32) != 0)
         return fail(c, LIM_ERR_ARG, "block_size must be a multiple of 32 in [32, 1024] (or 0)");
-    if (c->have_state && (q.dims != c->dims || q.pdim != c->pdim))
-        return fail(c, LIM_ERR_STATE, "dims/pdim differ from the uploaded state; upload the state again");
-    const bool fo_changed = c->have_state && q.freezeout_capture && !c->P.freezeout_capture;
+    // A state of another shape or precision, or without latch buffers (they are
+    // allocated at upload), no longer matches: it is dropped and must be uploaded again.
+    const bool stale = c->have_state &&
+        (q.dims != c->dims || q.pdim != c->pdim || (int)q.precision != c->state_prec ||
+         (q.freezeout_capture && !c->P.freezeout_capture));
     c->P = q;
     c->have_params = true;
-    if (fo_changed) c->have_state = false;   // latch buffers are allocated at upload
+    if (stale) c->have_state = false;
     return LIM_OK;
 }
 
@@ -623,6 +601,7 @@ int lim_set_medium_rt(lim_ctx* c, const double* xgrid, int64_t nr, const double*
                       const double* T, const double* V, const double* V2)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (!xgrid || !tgrid || !T || !V) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: NULL grid or field");
     if (nr < 2 || nt < 2) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: need at least 2 nodes per axis (got %lld x %lld)", (long long)nr, (long long)nt);
     if (!all_finite(xgrid, nr) || !all_finite(tgrid, nt)) return fail(c, LIM_ERR_ARG, "lim_set_medium_rt: non-finite grid node");
@@ -641,6 +620,7 @@ int lim_set_medium_rt(lim_ctx* c, const double* xgrid, int64_t nr, const double*
 int lim_set_medium_bjorken(lim_ctx* c, double T0, double tau0, double power, double r_max)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (!(T0 >= 0) || !(tau0 > 0) || !std::isfinite(power) || !std::isfinite(r_max))
         return fail(c, LIM_ERR_ARG, "lim_set_medium_bjorken: need T0 >= 0, tau0 > 0, finite power and r_max");
     c->bj_T0 = T0; c->bj_tau0 = tau0; c->bj_power = power; c->bj_rmax = r_max;
@@ -653,6 +633,7 @@ int lim_set_medium_grid(lim_ctx* c, int64_t nx, int64_t ny, int64_t nt, double x
                         double tau0, double dtau, const float* T, const float* ux, const float* uy)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (!T || !ux || !uy) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: NULL field");
     if (nx < 2 || ny < 2 || nt < 2) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: need at least 2 nodes per axis");
     if (!(dx > 0) || !(dy > 0) || !(dtau > 0)) return fail(c, LIM_ERR_ARG, "lim_set_medium_grid: spacings must be positive");
@@ -670,6 +651,7 @@ int lim_set_medium_grid(lim_ctx* c, int64_t nx, int64_t ny, int64_t nt, double x
 int lim_set_spline(lim_ctx* c, int which, double Tmin, double invdT, const double* vals, int64_t n)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (which != LIM_SPLINE_DRAG && which != LIM_SPLINE_RTA) return fail(c, LIM_ERR_ARG, "lim_set_spline: unknown spline %d", which);
     if (!vals || n < 1) return fail(c, LIM_ERR_ARG, "lim_set_spline: empty spline");
     if (!std::isfinite(Tmin) || !std::isfinite(invdT)) return fail(c, LIM_ERR_ARG, "lim_set_spline: non-finite Tmin/invdT");
@@ -683,6 +665,7 @@ int lim_set_spline(lim_ctx* c, int which, double Tmin, double invdT, const doubl
 int lim_set_invcdf(lim_ctx* c, const double* vals, int64_t nU, int64_t nT, double Tmin, double invdT)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (!vals || nU < 2 || nT < 2) return fail(c, LIM_ERR_ARG, "lim_set_invcdf: need nU >= 2 and nT >= 2");
     if (!std::isfinite(Tmin) || !std::isfinite(invdT)) return fail(c, LIM_ERR_ARG, "lim_set_invcdf: non-finite Tmin/invdT");
     c->icdf.assign(vals, vals + nU * nT);
@@ -694,6 +677,7 @@ int lim_set_invcdf(lim_ctx* c, const double* vals, int64_t nU, int64_t nT, doubl
 int lim_upload_state(lim_ctx* c, const double* x, int64_t dims, const double* p, int64_t pdim, int64_t n)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     int rc = state_rows_ok(c);
     if (rc) return rc;
     if (n < 0) return fail(c, LIM_ERR_ARG, "lim_upload_state: negative particle count");
@@ -851,6 +835,7 @@ int lim_observables(lim_ctx* c, int from_freezeout, double* out)
 int lim_record_noise(lim_ctx* c, int64_t first_step, int64_t nsteps)
 {
     if (!c) return LIM_ERR_ARG;
+    ++c->gen;
     if (nsteps <= 0) { dev_free(c->d_rec); c->rec_steps = 0; return LIM_OK; }
     if (!c->have_state) return fail(c, LIM_ERR_STATE, "upload the state before enabling noise recording");
     const double bytes = (double)nsteps * kNoiseSlots * (double)c->n * sizeof(double);

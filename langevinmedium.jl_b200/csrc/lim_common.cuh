@@ -44,13 +44,17 @@ struct MediumDev {
     R T_scale;
 };
 
+// 16-byte aligned and sized, so that a kernel can stage it in shared memory with
+// 128-bit copies.
 template <typename R>
-struct KParams {
+struct alignas(16) KParams {
     // run constants
     double dt, t0;
     R m, DsT, Tfo, psi2, sqrt_dt, dtR;
     int rel, collision, redshift, diffusion, reflect, integrator, fo_capture, fo_interp, stop_fo;
     uint32_t seed_lo, seed_hi;
+    uint2 rk[10];          // Philox round keys of the seed (kernel-parameter constants)
+    int spl_shared;        // drag and RTA splines share their T grid: one index for both
     int64_t pid_offset;
     int64_t n;
     int dims, pdim;
@@ -111,23 +115,43 @@ __device__ __forceinline__ int cell_index(const R* __restrict__ g, int n, R x, i
     return k > n - 2 ? n - 2 : k;
 }
 
-// transport.jl:231-253 — eval_tau_n_spline (0-based).
+// transport.jl:231-253 — eval_tau_n_spline (0-based), split into the cell/weight
+// lookup and the evaluation so that two splines on one T grid share the lookup.
+template <typename R> struct SplIdx { int i; R t; int mode; };   // mode: 0 normal, 1 first value, 2 zero
+
+template <typename R>
+__device__ __forceinline__ SplIdx<R> spline_index(R T, R Tmin, R invdT, int n)
+{
+    SplIdx<R> s;
+    s.i = 0; s.t = R(0);
+    if (n < 2) { s.mode = 1; return s; }
+    if (!isfinite(T)) { s.mode = 2; return s; }
+    s.mode = 0;
+    R u = (T - Tmin) * invdT;
+    R fl = floor(u);
+    s.i = fl < R(0) ? 0 : (fl > R(n - 2) ? n - 2 : (int)fl);
+    s.t = u - R(s.i);
+    return s;
+}
+
+template <typename R>
+__device__ __forceinline__ R spline_at(const R* __restrict__ vals, const SplIdx<R>& s)
+{
+    if (s.mode == 1) return __ldg(vals);
+    if (s.mode == 2) return R(0);
+    R y0 = __ldg(vals + s.i), y1 = __ldg(vals + s.i + 1);
+    if (sizeof(R) == 8) return (R(1) - s.t) * y0 + s.t * y1;   // the reference's form, for FP64 parity
+    return y0 + s.t * (y1 - y0);                               // FP32: no cancellation when |t| is large
+}
+
 template <typename R>
 __device__ __forceinline__ R eval_spline(R T, R Tmin, R invdT, const R* __restrict__ vals, int n)
 {
-    if (n < 2) return __ldg(vals);
-    if (!isfinite(T)) return R(0);
-    R u = (T - Tmin) * invdT;
-    R fl = floor(u);
-    int i = fl < R(0) ? 0 : (fl > R(n - 2) ? n - 2 : (int)fl);
-    R t = u - R(i);
-    R y0 = __ldg(vals + i), y1 = __ldg(vals + i + 1);
-    if (sizeof(R) == 8) return (R(1) - t) * y0 + t * y1;   // the reference's form, for FP64 parity
-    return y0 + t * (y1 - y0);                             // FP32: no cancellation when |t| is large
+    return spline_at(vals, spline_index(T, Tmin, invdT, n));
 }
 
 // ---------------------------------------------------------------------------
-// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter (pid, step, 2*tag+half, 0)
+// Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), counter (pid, step, tag, 0)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 {
@@ -141,58 +165,102 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
     return c;
 }
 
-__device__ __forceinline__ double u01_f64(uint32_t hi, uint32_t lo)
+// The same block with the round keys precomputed (k_r = key + r (W0, W1)): the keys
+// become constant operands instead of two additions per round.
+__device__ __forceinline__ uint4 philox4x32_10_rk(uint4 c, const uint2* __restrict__ rk)
 {
-    unsigned long long v = ((unsigned long long)hi << 32) | (unsigned long long)lo | 1ull;
-    return __ull2double_rz(v) * 0x1p-64;     // (0,1), exact truncation to 53 bits
-}
-__device__ __forceinline__ float u01_f32(uint32_t hi)
-{
-    return __uint2float_rz(hi | 1u) * 0x1p-32f;   // (0,1), tracks u01_f64 to 2^-23
-}
-
-template <typename R> struct Uni4 { R u[4]; };
-
-// Four uniforms of `tag` for (pid, step).  FP64 combines the high words of block
-// (tag, 0) with the low words of block (tag, 1); FP32 uses the high words only.
-template <typename R>
-__device__ __forceinline__ Uni4<R> uniforms4(uint32_t seed_lo, uint32_t seed_hi, uint32_t pid, uint32_t step, int tag);
-
-template <>
-__device__ __forceinline__ Uni4<double> uniforms4<double>(uint32_t slo, uint32_t shi, uint32_t pid, uint32_t step, int tag)
-{
-    uint2 key = make_uint2(slo, shi);
-    uint4 h = philox4x32_10(make_uint4(pid, step, 2u * tag, 0u), key);
-    uint4 l = philox4x32_10(make_uint4(pid, step, 2u * tag + 1u, 0u), key);
-    Uni4<double> r;
-    r.u[0] = u01_f64(h.x, l.x); r.u[1] = u01_f64(h.y, l.y);
-    r.u[2] = u01_f64(h.z, l.z); r.u[3] = u01_f64(h.w, l.w);
-    return r;
-}
-template <>
-__device__ __forceinline__ Uni4<float> uniforms4<float>(uint32_t slo, uint32_t shi, uint32_t pid, uint32_t step, int tag)
-{
-    uint4 h = philox4x32_10(make_uint4(pid, step, 2u * tag, 0u), make_uint2(slo, shi));
-    Uni4<float> r;
-    r.u[0] = u01_f32(h.x); r.u[1] = u01_f32(h.y); r.u[2] = u01_f32(h.z); r.u[3] = u01_f32(h.w);
-    return r;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ rk[r].x, lo1, hi0 ^ c.w ^ rk[r].y, lo0);
+    }
+    return c;
 }
 
-// Box–Muller: (sqrt(-2 ln u0) cos 2πu1, sqrt(-2 ln u0) sin 2πu1).
-__device__ __forceinline__ void box_muller(double u0, double u1, double& z0, double& z1)
+// A particle's noise stream: the seed's round keys and the particle id.  The keys are
+// passed apart from the rest of the parameters so that a kernel whose per-ensemble
+// parameters live in shared memory still reads them as kernel-parameter constants.
+struct NoiseKey { const uint2* rk; uint32_t pid; };
+
+// The four words of `tag` for (pid, step): one Philox block, counter (pid, step, tag, 0).
+__device__ __forceinline__ uint4 philox_words(const uint2* rk, uint32_t pid, uint32_t step, int tag)
 {
-    double rad = sqrt(-2.0 * log(u0));
-    double th = 6.283185307179586 * u1;
+    return philox4x32_10_rk(make_uint4(pid, step, (uint32_t)tag, 0u), rk);
+}
+
+// Uniform variates.  A word w stands for u = (w + 1/2) 2^-32 in (0, 1), the same value
+// in both precisions.  FP64 holds u exactly.  FP32 evaluates the steep maps (log u near
+// 1, the inverse normal CDF and the inverse Jüttner CDF near 0 and 1) on u folded about
+// 1/2: u = mag (lower half) or 1 - mag (upper half), with
+// mag = (2 min(w, ~w) + 1) 2^-33 in (0, 1/2], so both tails keep full relative precision.
+__device__ __forceinline__ double u_exact(uint32_t w) { return fma((double)w, 0x1p-32, 0x1p-33); }
+__device__ __forceinline__ bool u_upper(uint32_t w) { return (int32_t)w < 0; }
+
+template <typename R> __device__ __forceinline__ R u_mag(uint32_t w);
+template <> __device__ __forceinline__ double u_mag<double>(uint32_t w)
+{
+    const uint32_t m = u_upper(w) ? ~w : w;
+    return (double)(2u * m + 1u) * 0x1p-33;
+}
+template <> __device__ __forceinline__ float u_mag<float>(uint32_t w)
+{
+    const uint32_t m = u_upper(w) ? ~w : w;
+    return __uint2float_rn(2u * m + 1u) * 0x1p-33f;
+}
+
+template <typename R> __device__ __forceinline__ R u_value(uint32_t w);
+template <> __device__ __forceinline__ double u_value<double>(uint32_t w) { return u_exact(w); }
+template <> __device__ __forceinline__ float u_value<float>(uint32_t w)
+{
+    return fmaf(__uint2float_rn(w), 0x1p-32f, 0x1p-33f);
+}
+
+// -2 ln u.  FP32 upper half: ln(1 - mag) = ln(y) + r/y with y = fl(1 - mag) and the
+// exact rounding error r = (1 - mag) - y (Fast2Sum), so one logf serves both halves.
+__device__ __forceinline__ double neg2_log_u(uint32_t w, double) { return -2.0 * log(u_exact(w)); }
+__device__ __forceinline__ float neg2_log_u(uint32_t w, float)
+{
+    const float mag = u_mag<float>(w);
+    const bool up = u_upper(w);
+    const float y = 1.0f - mag;
+    const float r = -mag - (y - 1.0f);
+    const float a = up ? y : mag;
+    const float c = up ? __fdividef(r, y) : 0.0f;
+    return -2.0f * (logf(a) + c);
+}
+
+// 2u - 1 = (2w + 1 - 2^32) 2^-32, the Box–Muller angle in units of pi.
+__device__ __forceinline__ double u_centered(uint32_t w, double) { return fma((double)(int32_t)(w ^ 0x80000000u), 0x1p-31, 0x1p-32); }
+__device__ __forceinline__ float u_centered(uint32_t w, float)
+{
+    return fmaf(__int2float_rn((int32_t)(w ^ 0x80000000u)), 0x1p-31f, 0x1p-32f);
+}
+
+// Box–Muller with the angle in (-pi, pi): (rad cos(pi(2u1-1)), rad sin(pi(2u1-1))),
+// rad = sqrt(-2 ln u0).  FP32 uses the hardware sine/cosine, accurate to 2^-21.4
+// absolute on [-pi, pi].
+__device__ __forceinline__ void box_muller(uint32_t w0, uint32_t w1, double& z0, double& z1)
+{
+    const double rad = sqrt(neg2_log_u(w0, 0.0));
     double s, c;
-    sincos(th, &s, &c);
+    sincospi(u_centered(w1, 0.0), &s, &c);
     z0 = rad * c; z1 = rad * s;
 }
-__device__ __forceinline__ void box_muller(float u0, float u1, float& z0, float& z1)
+__device__ __forceinline__ void box_muller(uint32_t w0, uint32_t w1, float& z0, float& z1)
 {
-    float rad = sqrtf(-2.0f * logf(u0));
+    const float rad = sqrtf(neg2_log_u(w0, 0.0f));
     float s, c;
-    sincospif(2.0f * u1, &s, &c);
+    __sincosf(3.14159265358979f * u_centered(w1, 0.0f), &s, &c);
     z0 = rad * c; z1 = rad * s;
+}
+
+// Inverse standard normal CDF of u (FP32: of the folded magnitude, sign restored).
+__device__ __forceinline__ double norm_inv(uint32_t w, double) { return normcdfinv(u_exact(w)); }
+__device__ __forceinline__ float norm_inv(uint32_t w, float)
+{
+    const float z = normcdfinvf(u_mag<float>(w));
+    return u_upper(w) ? -z : z;
 }
 
 }  // namespace lim

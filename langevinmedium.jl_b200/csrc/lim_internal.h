@@ -31,6 +31,28 @@ template <typename R>
 cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, double width,
                                double* partials, int64_t nblocks_max, double* out, cudaStream_t st);
 
+// Batched persistent launch (lim_batch.cu): one launch advances every listed
+// (ensemble, tile) item through the chunk window [chunk_lo, chunk_lo + chunk_len),
+// counted from each ensemble's first step (KParams::step_base) and cut at its last.
+template <typename R>
+struct BatchLaunch {
+    const KParams<R>* ens;     // per-ensemble parameters (device)
+    const int2* items;         // this chunk's items: (ensemble, tile of blockDim particles)
+    unsigned* counter;         // this chunk's work counter, zero before the launch
+    int n_items;
+    int64_t chunk_lo, chunk_len;
+    uint2 rk[10];              // Philox round keys of the batch's seed
+};
+// cap: FP32 build capped at 64 registers (four 256-thread blocks per SM).
+template <typename R>
+cudaError_t launch_batch(const BatchLaunch<R>& bl, int dims, int pdim, bool fo, bool cap, int grid, int block,
+                         cudaStream_t st);
+template <typename R>
+cudaError_t batch_blocks_per_sm(int dims, int pdim, bool fo, bool cap, int block, int* out);
+// The per-step records of one ensemble, steps [s0, s0 + n), into `out`.
+template <typename R>
+cudaError_t launch_batch_table(const KParams<R>& kp, int64_t s0, int64_t n, void* out, cudaStream_t st);
+
 cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
 
 // FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.

@@ -8,45 +8,9 @@
 #include <climits>
 #include "lim_internal.h"
 #include "lim_step.cuh"
+#include "lim_particle.cuh"
 
 namespace lim {
-
-template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&x)[3], float (&xl)[3], double (&p)[3])
-{
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { x[d] = R(0); xl[d] = 0.f; p[d] = 0.0; }
-#pragma unroll
-    for (int d = 0; d < DIMS; ++d) {
-        x[d] = kp.x[d][i];
-        if (sizeof(R) == 4) xl[d] = kp.xlo[d][i];
-    }
-#pragma unroll
-    for (int d = 0; d < PDIM; ++d) p[d] = kp.p[d][i];
-}
-
-template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, const R (&x)[3], const float (&xl)[3], const double (&p)[3])
-{
-#pragma unroll
-    for (int d = 0; d < DIMS; ++d) {
-        kp.x[d][i] = x[d];
-        if (sizeof(R) == 4) kp.xlo[d][i] = xl[d];
-    }
-#pragma unroll
-    for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
-}
-
-template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ bool state_finite(const R (&x)[3], const double (&p)[3])
-{
-    bool ok = true;
-#pragma unroll
-    for (int d = 0; d < DIMS; ++d) ok &= (bool)isfinite(x[d]);
-#pragma unroll
-    for (int d = 0; d < PDIM; ++d) ok &= (bool)isfinite(p[d]);
-    return ok;
-}
 
 template <typename R, int MED>
 __global__ void k_step_table(const KParams<R> kp, int64_t s0, int64_t n)
@@ -62,39 +26,7 @@ k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kp.n) return;
-    R x[3];
-    double p[3];
-    float xl[3];
-    load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    double flag = 0.0, ltau = 0.0, lT = 0.0;
-    double lpos[3] = { 0.0, 0.0, 0.0 }, lmom[3] = { 0.0, 0.0, 0.0 };
-    if (FO) {
-        flag = kp.fo_flag[i]; ltau = kp.l_tau[i]; lT = kp.l_T[i];
-#pragma unroll
-        for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
-    }
-    const uint32_t pid = (uint32_t)(kp.pid_offset + i);
-    const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
-    for (int64_t s = s0; s < s1; ++s) {
-        if (FO && kp.stop_fo && flag != 0.0) break;
-        const StepRec<R> sr = tab[s];
-        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, pid, x, xl, p);
-        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT);
-        if (!state_finite<R, DIMS, PDIM>(x, p)) {
-            atomicMin(kp.first_bad, (unsigned long long)s);
-            break;
-        }
-    }
-    store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    if (FO) {
-        kp.l_tau[i] = ltau; kp.l_T[i] = lT;
-#pragma unroll
-        for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos[d];
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom[d];
-    }
+    cart_particle<REC, FO, R, MED, DIMS, PDIM>(kp, kp.rk, i, s0, s1);
 }
 
 template <bool REC, typename R>
@@ -107,11 +39,11 @@ k_milne(const KParams<R> kp, int64_t s0, int64_t s1)
     double p[3];
     float xl[3];
     load_state<R, 2, 2>(kp, i, x, xl, p);
-    const uint32_t pid = (uint32_t)(kp.pid_offset + i);
+    const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
     for (int64_t s = s0; s < s1; ++s) {
         const StepRec<R> sr = tab[s];
-        milne_step<REC, R>(kp, sr, i, s, pid, x, xl, p);
+        milne_step<REC, R>(kp, sr, i, s, nk, x, xl, p);
         if (!state_finite<R, 2, 2>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;

@@ -1,0 +1,88 @@
+// lim_particle.cuh — one particle through a range of Cartesian steps: state loaded
+// once, every step of the range evolved in registers, state stored once.  Shared by
+// the plain step kernel (one ensemble per launch) and the batched persistent kernel
+// (many ensembles per launch, parameters staged in shared memory).
+#pragma once
+#include "lim_step.cuh"
+
+namespace lim {
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ void load_state(const KParams<R>& kp, int64_t i, R (&x)[3], float (&xl)[3], double (&p)[3])
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { x[d] = R(0); xl[d] = 0.f; p[d] = 0.0; }
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) {
+        x[d] = kp.x[d][i];
+        if (sizeof(R) == 4) xl[d] = kp.xlo[d][i];
+    }
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) p[d] = kp.p[d][i];
+}
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, const R (&x)[3], const float (&xl)[3], const double (&p)[3])
+{
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) {
+        kp.x[d][i] = x[d];
+        if (sizeof(R) == 4) kp.xlo[d][i] = xl[d];
+    }
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
+}
+
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ bool state_finite(const R (&x)[3], const double (&p)[3])
+{
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) ok &= (bool)isfinite(x[d]);
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) ok &= (bool)isfinite(p[d]);
+    return ok;
+}
+
+// Steps [s0, s1) of particle i.  rk: the Philox round keys (kernel-parameter
+// constants in both kernels); kp: the ensemble's parameters.
+template <bool REC, bool FO, typename R, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2* __restrict__ rk, int64_t i,
+                                              int64_t s0, int64_t s1)
+{
+    R x[3];
+    double p[3];
+    float xl[3];
+    load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
+    double flag = 0.0, ltau = 0.0, lT = 0.0;
+    double lpos[3] = { 0.0, 0.0, 0.0 }, lmom[3] = { 0.0, 0.0, 0.0 };
+    if (FO) {
+        flag = kp.fo_flag[i]; ltau = kp.l_tau[i]; lT = kp.l_T[i];
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
+    }
+    const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
+    const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
+    for (int64_t s = s0; s < s1; ++s) {
+        if (FO && kp.stop_fo && flag != 0.0) break;
+        const StepRec<R> sr = tab[s];
+        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
+        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT);
+        if (!state_finite<R, DIMS, PDIM>(x, p)) {
+            atomicMin(kp.first_bad, (unsigned long long)s);
+            break;
+        }
+    }
+    store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
+    if (FO) {
+        kp.l_tau[i] = ltau; kp.l_T[i] = lT;
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos[d];
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom[d];
+    }
+}
+
+}  // namespace lim

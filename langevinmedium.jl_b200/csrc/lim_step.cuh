@@ -8,9 +8,9 @@
 //
 // Variates per step (counter-based Philox, see lim_common.cuh), slot numbers as
 // recorded by the noise-recording mode:
-//   group MOM  u0..u3: momentum normals (u0,u1)->(xi0,xi1), (u2,u3)->(xi2,z3);
-//                      RTA decision u_collide = Phi(z3) when pdim = 3, u2 when
-//                      pdim < 3, u0 in pure RTA mode                   [slots 0-3]
+//   group MOM  u0..u3: momentum normals (u0,u1) -> Box-Muller (xi0,xi1),
+//                      xi2 = Phi^-1(u2); RTA decision u_collide = u3 when pdim = 3,
+//                      u2 when pdim < 3, u0 in pure RTA mode           [slots 0-3]
 //   group RTA  (drawn only when a collision happens): u_sample = u0,
 //                      (u1,u2) -> directions g0, g1                    [slots 4-6]
 //   group RTADIR (pdim = 3 collisions): (u0,u1) -> g2                  [slot 7]
@@ -27,14 +27,14 @@ namespace lim {
 template <typename R>
 struct __align__(16) StepRec {
     double t;    // medium time s*dt + t0
-    R tR;        // the same in R
-    R wt;        // time weight of the (r,t) table, the grid or the Milne table
-    R T_bj;      // Bjorken temperature at t
-    R zf;        // Bjorken redshift factor tau_a/(tau_a+dt), 1 when not applied
-    int kt;      // time cell
-    int pad;
+    double zf;   // Bjorken redshift factor tau_a/(tau_a+dt), 1 when not applied (FP64:
+                 // the product over steps telescopes to tau_0/tau exactly)
     double wtd;  // time weight in FP64
     double Td;   // Bjorken temperature in FP64
+    R tR;        // the medium time in R
+    R wt;        // time weight of the (r,t) table, the grid or the Milne table
+    R T_bj;      // Bjorken temperature at t
+    int kt;      // time cell
 };
 
 enum { MED_MILNE_TABLE = 3 };   // Milne (tau, r): unclamped time interpolation
@@ -45,7 +45,7 @@ __device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_
     StepRec<R> u;
     u.t = __dadd_rn(__dmul_rn((double)s, kp.dt), kp.t0);
     u.tR = (R)u.t;
-    u.kt = 0; u.pad = 0; u.wt = R(0); u.T_bj = R(0); u.zf = R(1); u.wtd = 0.0; u.Td = 0.0;
+    u.kt = 0; u.wt = R(0); u.T_bj = R(0); u.zf = 1.0; u.wtd = 0.0; u.Td = 0.0;
     const MediumDev<R>& md = kp.med;
     if (MED == MED_RT || MED == MED_MILNE_TABLE) {
         const double* tg = md.tgd;
@@ -77,7 +77,7 @@ __device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_
     }
     if (kp.redshift) {                 // kernels_cpu.jl:427-435
         double ta = kp.t0 + (double)(s - 1) * kp.dt;
-        if (ta > 0.0) u.zf = (R)(ta / (ta + kp.dt));
+        if (ta > 0.0) u.zf = ta / (ta + kp.dt);
     }
     return u;
 }
@@ -252,7 +252,7 @@ __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, d
 
 // Records a consumed variate (noise-recording instantiation only).
 template <bool REC, typename R>
-__device__ __forceinline__ void rec_slot(const KParams<R>& kp, int64_t s, int64_t i, int slot, R val)
+__device__ __forceinline__ void rec_slot(const KParams<R>& kp, int64_t s, int64_t i, int slot, double val)
 {
     if (REC && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
         kp.rec[((s - kp.rec_first) * kNoiseSlots + slot) * kp.n + i] = (double)val;
@@ -275,12 +275,11 @@ __device__ __forceinline__ float expm1_neg(float x)
 }
 
 // kernels_cpu.jl:246-357 + :406-417: exact-OU drag and kick in the LRF.
+// tau: the drag time from the drag spline (0 when DsT <= 0), kernels_cpu.jl:270-281.
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, double (&p)[3], const R (&xi)[3])
+__device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, R tau, double (&p)[3], const R (&xi)[3])
 {
     const R M = kp.m, dt = kp.dtR;
-    const R DsT_safe = kp.DsT <= R(0) ? R(0) : kp.DsT;
-    R tau = DsT_safe == R(0) ? R(0) : eval_spline(T, kp.drag_Tmin, kp.drag_invdT, kp.drag, kp.n_drag);
     const bool ok = tau > R(0) && isfinite(tau);
     if (sizeof(R) == 4) {
         // FP32: with kappa = 2MT/tau and eta_eff = (M/E)/tau the kick amplitude
@@ -353,19 +352,23 @@ __device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, double 
     for (int d = 0; d < PDIM; ++d) p[d] += (a - R(1)) * p[d] + kp.sqrt_dt * (np * xi[d]);
 }
 
-// kernels_gpu.jl:88-117
+// kernels_gpu.jl:88-117.  The u-cell is located from the nearer end of the u grid
+// (u or 1 - u, both exact), so the steep tail cells of p*(u) near u = 1 are resolved as
+// finely as those near 0; FP32 adds the FMA residual of mag*(nU-1), which restores the
+// cell weight exactly.
 template <typename R>
-__device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, R u, R T)
+__device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, uint32_t w, R T)
 {
     const int nU = kp.nU, nT = kp.nT;
-    R uu = u < R(0) ? R(0) : (u > R(1) ? R(1) : u);
-    R fu = uu * R(nU - 1);
-    int iu = (int)floor(fu);
+    const R mag = u_mag<R>(w);
+    const R fm = mag * R(nU - 1);
+    const R k = floor(fm);
+    R fr = fm - k;
+    if (sizeof(R) == 4) fr += fma(mag, R(nU - 1), -fm);
+    const bool up = u_upper(w);
+    int iu = up ? nU - 2 - (int)k : (int)k;
     iu = iu < 0 ? 0 : (iu > nU - 2 ? nU - 2 : iu);
-    R tu = fu - R(iu);
-    // FP32: u*(nU-1) rounds away up to 2^-24 (nU-1) of the cell weight, which the steep
-    // tail of p*(u) turns into a 1e-5 error; the FMA residual restores it exactly.
-    if (sizeof(R) == 4) tu += fma(uu, R(nU - 1), -fu);
+    const R tu = up ? R(1) - fr : fr;
     R fT = (T - kp.ic_Tmin) * kp.ic_invdT;
     R flT = floor(fT);
     int jT = flT < R(0) ? 0 : (flT > R(nT - 2) ? nT - 2 : (int)flT);
@@ -383,24 +386,24 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, R u, R T)
 // from the Jüttner inverse CDF and an isotropic direction.  The collision
 // uniform u_collide comes with the step's momentum variates; the sample and the
 // direction are drawn only when the particle collides.
+// tn: the RTA relaxation time (0 when DsT <= 0 or T <= 0), kernels_gpu.jl:675-679.
 template <bool REC, typename R, int DIMS, int PDIM>
-__device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, uint32_t pid,
-                                            R T, R uc, double (&p)[3])
+__device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, const NoiseKey& nk,
+                                            R T, R tn, R uc, double (&p)[3])
 {
-    R tn = (kp.DsT > R(0) && T > R(0)) ? eval_spline(T, kp.rta_Tmin, kp.rta_invdT, kp.rta, kp.n_rta) : R(0);
     R Pcol = (tn > R(0) && isfinite(tn)) ? jclamp(kp.dtR / tn, R(0), R(1)) : R(1);
     if (!(uc < Pcol || Pcol >= R(1))) return;
-    Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_RTA);
-    R pstar = invcdf_lookup(kp, u.u[0], T);
+    const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTA);
+    R pstar = invcdf_lookup(kp, u.x, T);
     R g[3];
-    box_muller(u.u[1], u.u[2], g[0], g[1]);
+    box_muller(u.y, u.z, g[0], g[1]);
     g[2] = R(0);
     if (PDIM == 3) {
-        Uni4<R> w = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_RTADIR);
+        const uint4 v = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTADIR);
         R z;
-        box_muller(w.u[0], w.u[1], g[2], z);
+        box_muller(v.x, v.y, g[2], z);
     }
-    rec_slot<REC>(kp, s, i, 4, u.u[0]);
+    rec_slot<REC>(kp, s, i, 4, u_exact(u.x));
 #pragma unroll
     for (int d = 0; d < 3; ++d) rec_slot<REC>(kp, s, i, 5 + d, g[d]);
     if (DIMS == 1) { p[0] = (double)((g[0] < R(0) ? R(-1) : R(1)) * pstar); return; }
@@ -473,7 +476,7 @@ __device__ __forceinline__ void acc_add(R& hi, float& lo, R dx)
 // kernels_cpu.jl:510-637
 template <bool REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
-                                                 uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
+                                                 const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
     const R m = kp.m, dt = kp.dtR;
     R pr_[3];
@@ -494,9 +497,9 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
             R T = temperature_at<R, MED, DIMS>(kp, sr, xs, r_safe);
             R D = (kp.DsT / (T != T ? T : (T > R(kEps) ? T : R(kEps)))) / R(kFmGeV);
             if (D > R(0)) {
-                Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_DIFF);
+                const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_DIFF);
                 R z0, z1;
-                box_muller(u.u[0], u.u[1], z0, z1);
+                box_muller(u.x, u.y, z0, z1);
                 rec_slot<REC>(kp, s, i, 8, z0);
                 dr += (D / r_safe) * dt + sqrt(R(2) * D * dt) * z0;
             }
@@ -525,10 +528,10 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
         R D = (kp.DsT / (T != T ? T : (T > R(kEps) ? T : R(kEps)))) / R(kFmGeV);
         if (D > R(0)) {
             R sg = sqrt(R(2) * D * dt);
-            Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_DIFF);
+            const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_DIFF);
             R z[4];
-            box_muller(u.u[0], u.u[1], z[0], z[1]);
-            box_muller(u.u[2], u.u[3], z[2], z[3]);
+            box_muller(u.x, u.y, z[0], z[1]);
+            box_muller(u.z, u.w, z[2], z[3]);
 #pragma unroll
             for (int d = 0; d < DIMS; ++d) { rec_slot<REC>(kp, s, i, 8 + d, z[d]); acc_add(x[d], xl[d], sg * z[d]); }
         }
@@ -555,38 +558,46 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
 // One Cartesian step (simulate_cpu.jl:215-290).
 template <bool REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
-                                          uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
+                                          const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
     const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x);
     if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, false);
-    if (PDIM == 3 && kp.redshift) p[2] *= (double)sr.zf;
+    if (PDIM == 3 && kp.redshift) p[2] *= sr.zf;
     if (kp.collision == COLL_FLUID) {
         set_to_fluid<R, MED, DIMS>(kp, sr, x, p);
     } else {
         const R T = jmax0(L.T);
-        const Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_MOM);
-        R uc = u.u[0];
-        if (kp.collision != COLL_RTA) {
-            R xi[3], z3;
-            box_muller(u.u[0], u.u[1], xi[0], xi[1]);
+        const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_MOM);
+        const bool kick = kp.collision != COLL_RTA;
+        const bool rta = kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA;
+        // one T-grid lookup for both splines when they share the grid
+        const SplIdx<R> sd = spline_index(T, kp.drag_Tmin, kp.drag_invdT, kp.n_drag);
+        uint32_t wc = u.x;                   // the collision word
+        if (kick) {
+            R xi[3];
+            box_muller(u.x, u.y, xi[0], xi[1]);
             if (PDIM == 3) {
-                box_muller(u.u[2], u.u[3], xi[2], z3);
-                if (kp.collision == COLL_LANGEVIN_RTA) uc = normcdf(z3);
+                xi[2] = norm_inv(u.z, R(0));
+                wc = u.w;
             } else {
                 xi[2] = R(0);
-                uc = u.u[2];
+                wc = u.z;
             }
 #pragma unroll
             for (int d = 0; d < PDIM; ++d) rec_slot<REC>(kp, s, i, d, xi[d]);
-            langevin_kick<R, DIMS, PDIM>(kp, T, p, xi);
+            const R tau = kp.DsT <= R(0) ? R(0) : spline_at(kp.drag, sd);
+            langevin_kick<R, DIMS, PDIM>(kp, T, tau, p, xi);
         }
-        if (kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA) {
-            rec_slot<REC>(kp, s, i, 3, uc);
-            rta_collide<REC, R, DIMS, PDIM>(kp, i, s, pid, T, uc, p);
+        if (rta) {
+            rec_slot<REC>(kp, s, i, 3, u_exact(wc));
+            R tn = R(0);
+            if (kp.DsT > R(0) && T > R(0))
+                tn = spline_at(kp.rta, kp.spl_shared ? sd : spline_index(T, kp.rta_Tmin, kp.rta_invdT, kp.n_rta));
+            rta_collide<REC, R, DIMS, PDIM>(kp, i, s, nk, T, tn, u_value<R>(wc), p);
         }
         if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true);
     }
-    stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, pid, x, xl, p);
+    stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
 }
 
 // Temperature at the particle in FP64 arithmetic (FP64 weights over the stored
@@ -716,7 +727,7 @@ __device__ __forceinline__ void milne_lookup(const MediumDev<R>& md, const StepR
 
 template <bool REC, typename R>
 __device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
-                                           uint32_t pid, R (&x)[3], float (&xl)[3], double (&p)[3])
+                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
     const double m = (double)kp.m;
     const R dt = kp.dtR;
@@ -736,9 +747,9 @@ __device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepRec<R
     R etaD = ok ? R(1) / tn : R(0);
     R kappa = ok ? (R(2) * kp.m * T) / tn : R(0);
     R kT = sqrt(kappa);
-    Uni4<R> u = uniforms4<R>(kp.seed_lo, kp.seed_hi, pid, (uint32_t)s, TAG_MOM);
+    const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_MOM);
     R xi, z1;
-    box_muller(u.u[0], u.u[1], xi, z1);
+    box_muller(u.x, u.y, xi, z1);
     rec_slot<REC>(kp, s, i, 0, xi);
     if (sizeof(R) == 8) {
         R det, sto;

@@ -18,6 +18,7 @@
  * counter-based Philox-4x32-10 stream keyed by (seed, particle, step, tag),
  * which the CUDA engine draws from too.
  */
+#define _GNU_SOURCE
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -155,15 +156,23 @@ static double eval_spline(double T, double Tmin, double invdT, const double* val
     return (1.0 - t) * y0 + t * y1;
 }
 
-/* kernels_gpu.jl:88-117 — bilinear lookup of the Jüttner inverse CDF. */
+/* kernels_gpu.jl:88-117 — bilinear lookup of the Jüttner inverse CDF.  The u-cell is
+ * located from the nearer end of the u grid: with mag = min(u, 1-u) (exact for u in
+ * (0,1)), position mag (nU-1) counted from u = 0 or from u = 1.  In exact arithmetic
+ * this is u (nU-1); it keeps the steep cells near u = 1 as finely resolved as those
+ * near 0. */
 static double invcdf_lookup(const orc_medium* md, double u, double T)
 {
     int64_t nU = md->nU, nT = md->nT;
     double uu = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
-    double fu = uu * (double)(nU - 1);
-    int64_t iu = (int64_t)floor(fu);
+    const int up = uu > 0.5;
+    double mag = up ? 1.0 - uu : uu;
+    double fm = mag * (double)(nU - 1);
+    double k = floor(fm);
+    double fr = fm - k;
+    int64_t iu = up ? nU - 2 - (int64_t)k : (int64_t)k;
     iu = iu < 0 ? 0 : (iu > nU - 2 ? nU - 2 : iu);
-    double tu = fu - (double)iu;
+    double tu = up ? 1.0 - fr : fr;
     double fT = (T - md->ic_Tmin) * md->ic_invdT;
     int64_t jT = (int64_t)floor(fT);
     jT = jT < 0 ? 0 : (jT > nT - 2 ? nT - 2 : jT);
@@ -202,60 +211,72 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* Keep the top `bits` significant bits of v (round toward zero), so that the
- * conversion to floating point is exact. */
-static inline uint64_t trunc_bits64(uint64_t v, int bits)
-{
-    int lead = 63 - __builtin_clzll(v);
-    if (lead >= bits) v &= ~((UINT64_C(1) << (lead - bits + 1)) - 1);
-    return v;
-}
-/* FP64 uniform in (0,1) from a (hi, lo) word pair. */
-static inline double u01_f64(uint32_t hi, uint32_t lo)
-{
-    uint64_t v = ((uint64_t)hi << 32) | (uint64_t)lo | UINT64_C(1);
-    return (double)trunc_bits64(v, 53) * 0x1p-64;
-}
-/* FP32 uniform in (0,1) from one word (what the FP32 kernel computes). */
-static inline double u01_f32(uint32_t hi)
-{
-    uint64_t v = (uint64_t)(hi | 1u);
-    return (double)(float)((double)trunc_bits64(v, 24) * 0x1p-32);
-}
+/* Uniform in (0,1) from one Philox word: u = (w + 1/2) 2^-32, exact in double.  Both
+ * precisions of the engine consume this same value. */
+static inline double u01(uint32_t w) { return ((double)w + 0.5) * 0x1p-32; }
 
-/* Four uniforms of tag `tag` for (particle, step): FP64 takes the high words
- * from block (tag,0) and the low words from block (tag,1); FP32 takes the high
- * words only, so FP32 variates track the FP64 ones to 2^-23 relative. */
+/* Four uniforms of tag `tag` for (particle, step): one Philox-4x32-10 block with
+ * counter (pid, step, tag, 0) and the 64-bit seed as key. */
 static void uniforms4(const orc_params* P, int64_t pid, int64_t step, int tag, double u[4])
 {
     uint32_t key[2] = { (uint32_t)(uint64_t)P->seed, (uint32_t)((uint64_t)P->seed >> 32) };
-    uint32_t ctr[4] = { (uint32_t)pid, (uint32_t)step, (uint32_t)(2 * tag), 0u };
-    uint32_t hi[4], lo[4];
-    orc_philox4x32_10(ctr, key, hi);
-    if (P->precision == 1) {
-        for (int k = 0; k < 4; ++k) u[k] = u01_f32(hi[k]);
-        return;
-    }
-    ctr[2] = (uint32_t)(2 * tag + 1);
-    orc_philox4x32_10(ctr, key, lo);
-    for (int k = 0; k < 4; ++k) u[k] = u01_f64(hi[k], lo[k]);
+    uint32_t ctr[4] = { (uint32_t)pid, (uint32_t)step, (uint32_t)tag, 0u };
+    uint32_t w[4];
+    orc_philox4x32_10(ctr, key, w);
+    for (int k = 0; k < 4; ++k) u[k] = u01(w[k]);
 }
+/* Box-Muller with the angle in (-pi, pi): (rad cos(pi(2u1-1)), rad sin(pi(2u1-1))). */
 static inline void box_muller(double u0, double u1, double* z0, double* z1)
 {
-    const double two_pi = 6.283185307179586;
     double rad = sqrt(-2.0 * log(u0));
-    double th = two_pi * u1;
+    double th = M_PI * (2.0 * u1 - 1.0);
     *z0 = rad * cos(th);
     *z1 = rad * sin(th);
 }
 
+/* Inverse standard normal CDF: P. J. Acklam's rational approximation (relative error
+ * 1.15e-9) refined by two Halley steps on erfc, which brings it to double precision. */
+static double norm_inv(double p)
+{
+    static const double a[6] = { -3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                                 1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00 };
+    static const double b[5] = { -5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                                 6.680131188771972e+01, -1.328068155288572e+01 };
+    static const double c[6] = { -7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                                 -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00 };
+    static const double d[4] = { 7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+                                 3.754408661907416e+00 };
+    const double plow = 0.02425;
+    /* work on the lower half: pl = min(p, 1-p) is exact for the (0,1) uniforms used here,
+     * and the Halley residual Phi(x) - pl then has no cancellation */
+    const int upper = p > 0.5;
+    const double pl = upper ? 1.0 - p : p;
+    double x;
+    if (pl < plow) {
+        double q = sqrt(-2.0 * log(pl));
+        x = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+            ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+    } else {
+        double q = pl - 0.5, r = q * q;
+        x = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+            (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+    }
+    for (int it = 0; it < 2; ++it) {
+        double e = 0.5 * erfc(-x / M_SQRT2) - pl;
+        double u = e * sqrt(2.0 * M_PI) * exp(0.5 * x * x);
+        x = x - u / (1.0 + 0.5 * x * u);
+    }
+    return upper ? -x : x;
+}
+double orc_norm_inv(double p) { return norm_inv(p); }
+
 /* Per-step variates of one particle, slot layout shared with the engine:
  *   0..2 momentum normals, 3 u_collide, 4 u_sample, 5..7 RTA direction
  *   normals, 8..10 position-diffusion normals.
- * Group MOM: (u0,u1) -> (xi0, xi1), (u2,u3) -> (xi2, z3).  The collision uniform is
- * Phi(z3) when pdim = 3 (z3 is independent of xi0..xi2), u2 when pdim < 3, and u0
- * when there is no Langevin kick.  Group RTA (only when a particle collides):
- * u_sample = u0, (u1,u2) -> (g0, g1); group RTADIR: (u0,u1) -> g2. */
+ * Group MOM: (u0,u1) -> Box-Muller (xi0, xi1); xi2 = Phi^-1(u2) when pdim = 3.  The
+ * collision uniform is u3 when pdim = 3, u2 when pdim < 3, and u0 when there is no
+ * Langevin kick.  Group RTA (only when a particle collides): u_sample = u0,
+ * (u1,u2) -> (g0, g1); group RTADIR: (u0,u1) -> g2. */
 typedef struct noise_src {
     const double* rec;      /* recorded buffer or NULL (Philox) */
     int64_t rec_first, rec_steps, n;
@@ -274,13 +295,13 @@ static void draw_step(const orc_params* P, const noise_src* ns, int64_t i, int64
         *uc = rec_at(ns, i, step, 3);
         return;
     }
-    double u[4], z3 = 0.0;
+    double u[4];
     uniforms4(P, P->particle_offset + i, step, TAG_MOM, u);
     if (!kick) { xi[0] = xi[1] = xi[2] = 0.0; *uc = u[0]; return; }
     box_muller(u[0], u[1], &xi[0], &xi[1]);
     if (P->pdim == 3) {
-        box_muller(u[2], u[3], &xi[2], &z3);
-        *uc = 0.5 * erfc(-z3 * 0.70710678118654752440);
+        xi[2] = norm_inv(u[2]);
+        *uc = u[3];
     } else {
         xi[2] = 0.0;
         *uc = u[2];

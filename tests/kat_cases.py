@@ -36,21 +36,29 @@ def case_equilibria(box_run):
     return e3, e2
 
 
-def case_l1_decay(box_run):
-    """(D) test_momentum_dims3.jl:145-171."""
+def case_l1_decay(box_run, N_D=200_000):
+    """(D) test_momentum_dims3.jl:145-171, with common random numbers: the unboosted
+    Jüttner sample is run with the identical noise stream and the decay of
+    <p_x>_boosted - <p_x>_unboosted is fitted.  Both have the expectation of the
+    boosted run (the unboosted one averages to zero), but the kick noise cancels: the
+    plain estimator's seed-to-seed spread is ±3.4 % against the 4 % gate, the
+    difference's is ±0.04 %."""
     v = 0.05
     g = 1 / math.sqrt(1 - v * v)
-    N_D = 400_000
     rates, refs = {}, {}
     for d in (3, 2):
-        P = juttner_sample(np.random.default_rng(100 + d), M_, T_, d, N_D)
+        P0 = juttner_sample(np.random.default_rng(100 + d), M_, T_, d, N_D)
+        P = P0.copy()
         E = np.sqrt(M_ ** 2 + np.sum(P ** 2, axis=0))
         P[0] = g * (P[0] + v * E)
-        tt, mm, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_D, dt=1e-3, tfinal=0.30, save=0.05,
-                            x0=np.zeros((2, N_D)), p0=P, pdim=d, seed=5 + d)
-        jx = np.array([est(m, M_)["jx"] for m in mm])
+        runs = []
+        for Pin in (P, P0):
+            tt, mm, _ = box_run(M=M_, T=T_, DsT=DST_, N=N_D, dt=1e-3, tfinal=0.30, save=0.05,
+                                x0=np.zeros((2, N_D)), p0=Pin, pdim=d, seed=5 + d)
+            runs.append(mm)
+        jx = np.array([est(a, M_)["jx"] - est(b, M_)["jx"] for a, b in zip(*runs)])
         tt = np.asarray(tt)
-        r_inst = ETA_ * est(mm[0], M_)["jxw"] / est(mm[0], M_)["jx"]
+        r_inst = ETA_ * est(runs[0][0], M_)["jxw"] / est(runs[0][0], M_)["jx"]
         A = np.vstack([np.ones_like(tt), tt]).T
         c = np.linalg.lstsq(A, np.log(jx), rcond=None)[0]
         rates[d] = -c[1]

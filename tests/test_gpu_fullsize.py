@@ -1,0 +1,102 @@
+"""Full-size checks on the GPU (1e6 particles), through properties that do not need
+the CPU restatement to finish at that size: FP32 against the FP64 engine on identical
+counter-based noise (the FP64 engine is pinned to the restatement at 1e-12 by
+test_gpu_parity), exact Bjorken telescoping, the ensemble drag decay of the exact OU
+process, and relaxation to the Jüttner distribution with its statistical error."""
+import math
+
+import numpy as np
+import pytest
+from scipy.special import kve
+
+from helpers import parity
+
+pytestmark = pytest.mark.gpu
+
+
+def run_final(lmb, wl, steps=None):
+    eng = lmb.capi.Engine(0)
+    lmb.workloads.configure(eng, wl)
+    if wl.params.get("coords", 0) == 0:
+        eng.initial_lab_boost()
+    eng.run(wl.first_step, steps or wl.steps)
+    x, p = eng.download_state()
+    obs = eng.observables()
+    eng.close()
+    return x, p, obs
+
+
+def test_fp32_vs_fp64_bjorken_full_size(lmb):
+    """The benchmark workload (1e6 charm, 1880 steps, Langevin + RTA) in FP32 against
+    FP64 on the same noise: per-particle error <= 1e-5 except particles whose RTA
+    decision flipped (u within FP32 rounding of the collision probability)."""
+    W = lmb.workloads
+    x32, p32, o32 = run_final(lmb, W.bjorken(N=1_000_000, precision="fp32"))
+    x64, p64, o64 = run_final(lmb, W.bjorken(N=1_000_000, precision="fp64"))
+    ep = np.linalg.norm(p32 - p64, axis=0) / np.maximum(np.linalg.norm(p64, axis=0), 0.3)
+    ex = np.linalg.norm(x32 - x64, axis=0) / np.maximum(np.linalg.norm(x64, axis=0), 1.0)
+    e = np.maximum(ep, ex)
+    flipped = int(np.count_nonzero(e > 1e-3))          # an O(1) jump: a different RTA decision
+    print(f"fp32 vs fp64 at 1e6: p99 {np.percentile(e, 99):.3g} p99.99 {np.percentile(e, 99.99):.3g} "
+          f"max(non-flipped) {e[e <= 1e-3].max():.3g} flipped {flipped}")
+    assert flipped <= 5
+    assert np.percentile(e, 99.99) <= 1e-5
+    assert e[e <= 1e-3].max() <= 1e-5
+    for k in ("mean_pt", "mean_p2", "mean_E"):
+        assert math.isclose(o32[k], o64[k], rel_tol=1e-5)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_bjorken_telescoping_full_size(lmb, prec):
+    """kernels_cpu.jl:427-435 with momentum_langevin=false: <p_z^2>(tau) = <p_z^2>(tau0)(tau0/tau)^2."""
+    W = lmb.workloads
+    capi = lmb.capi
+    wl = W.bjorken(N=1_000_000, precision=prec, steps=1880)
+    wl.params["collision"] = capi.LIM_COLL_FLUID
+    pz0 = wl.p[2].copy()
+    # the step-0 boost does not touch p_z; after s steps tau = tau0 + s dt
+    x, p, _ = run_final(lmb, wl)
+    tau = wl.params["t0"] + wl.steps * wl.params["dt"]
+    ratio = np.mean(p[2] ** 2) / np.mean(pz0 ** 2)
+    assert math.isclose(ratio, (wl.params["t0"] / tau) ** 2, rel_tol=1e-9)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_drag_decay_of_the_mean(lmb, prec):
+    """Non-relativistic exact OU: <p>(t) = p0 exp(-eta_D t) exactly in expectation
+    (the noise has zero mean); checked at 4 sigma of the ensemble's statistical error."""
+    W = lmb.workloads
+    wl = W.static_box(N=1_000_000, steps=300, precision=prec)
+    wl.params["relativistic"] = 0
+    wl.x[:] = 0.0                                         # r < eps: no frame change
+    wl.p[:] = np.array([[2.0], [-1.0], [0.5]])
+    m, T, DsT, dt = wl.params["m"], 0.30, wl.params["DsT"], wl.params["dt"]
+    eta = T * T / (m * DsT) / 0.197327                    # 1/tau_drag, transport.jl:132-137
+    x, p, _ = run_final(lmb, wl)
+    t = wl.steps * dt
+    a = math.exp(-eta * t)
+    var = m * T * (1 - a * a)                             # per component
+    for d, p0 in enumerate((2.0, -1.0, 0.5)):
+        assert abs(np.mean(p[d]) - p0 * a) <= 4 * math.sqrt(var / p.shape[1])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_juttner_relaxation_full_size(lmb, prec):
+    """Static medium, 3-D, the static-box initial state (|p| uniform in [0, 10] GeV):
+    relaxes to <p^2> = 3 M T K3/K2 and <E> = M K1/K2 + 3T within 3 sigma of the
+    ensemble error.  A 10 GeV charm quark loses ~0.48 GeV/fm and then relaxes at
+    ~0.5/fm, so the check runs 120 fm (12000 steps of 0.01 fm); at 40 fm the hot tail
+    still holds a few 1e-3 of <p^2>."""
+    W = lmb.workloads
+    wl = W.static_box(N=1_000_000, steps=12_000, precision=prec)
+    x, p, _ = run_final(lmb, wl)
+    m, T = wl.params["m"], 0.30
+    z = m / T
+    p2 = np.sum(p * p, axis=0)
+    E = np.sqrt(m * m + p2)
+    p2_ref = 3 * m * T * kve(3, z) / kve(2, z)
+    E_ref = m * kve(1, z) / kve(2, z) + 3 * T
+    print(f"juttner {prec}: <p2> {p2.mean():.5f} ref {p2_ref:.5f} sigma {p2.std() / math.sqrt(p2.size):.5f}; "
+          f"<E> {E.mean():.5f} ref {E_ref:.5f} sigma {E.std() / math.sqrt(E.size):.5f}")
+    assert abs(p2.mean() - p2_ref) <= 3 * p2.std() / math.sqrt(p2.size)
+    assert abs(E.mean() - E_ref) <= 3 * E.std() / math.sqrt(E.size)
