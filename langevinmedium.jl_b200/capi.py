@@ -53,6 +53,14 @@ _FP = C.POINTER(C.c_float)
 _U32P = C.POINTER(C.c_uint32)
 _I64P = C.POINTER(C.c_int64)
 
+class LimBatchShape(C.Structure):
+    """lim_batch_shape: block, chunk_steps, blocks_per_sm, reg_cap (0 = automatic)."""
+    _fields_ = [(n, C.c_int64) for n in ("block", "chunk_steps", "blocks_per_sm", "reg_cap")]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 _SIGS = {
     "lim_abi_version": ([], C.c_int),
     "lim_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
@@ -83,6 +91,15 @@ _SIGS = {
     "lim_probe_fma_rate": ([C.c_void_p, _DP, _DP], C.c_int),
     "lim_observables_noalloc": ([C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_double,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
+    "lim_batch_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "lim_batch_destroy": ([C.c_void_p], C.c_int),
+    "lim_batch_last_error": ([C.c_void_p], C.c_char_p),
+    "lim_batch_add": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, _I64P], C.c_int),
+    "lim_batch_set_shape": ([C.c_void_p, C.POINTER(LimBatchShape)], C.c_int),
+    "lim_batch_get_shape": ([C.c_void_p, C.POINTER(LimBatchShape)], C.c_int),
+    "lim_batch_run": ([C.c_void_p], C.c_int),
+    "lim_batch_tune": ([C.c_void_p, C.POINTER(LimBatchShape), _DP], C.c_int),
+    "lim_batch_stats": ([C.c_void_p, _DP, _I64P, _I64P], C.c_int),
 }
 
 
@@ -319,3 +336,64 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.lim_synchronize(self.ctx))
+
+
+class Batch:
+    """Many engine contexts advanced together (lim_batch_*): one persistent launch per
+    chunk of steps, the chunk loop replayed as a CUDA graph.  The engines are
+    referenced, not copied; keep them open while the batch lives."""
+
+    def __init__(self, device: int = 0, stream: int | None = None, lib: C.CDLL | None = None):
+        self.lib = lib or load_library()
+        self.h = C.c_void_p()
+        rc = self.lib.lim_batch_create(int(device), C.c_void_p(stream) if stream else None, C.byref(self.h))
+        if rc != LIM_OK:
+            raise LimError(rc, self.lib.lim_batch_last_error(None).decode())
+        self.engines = []
+
+    def _check(self, rc: int):
+        if rc != LIM_OK:
+            raise LimError(rc, self.lib.lim_batch_last_error(self.h).decode())
+
+    def close(self):
+        if self.h:
+            self.lib.lim_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, engine: Engine, first_step: int, nsteps: int) -> int:
+        idx = C.c_int64(-1)
+        self._check(self.lib.lim_batch_add(self.h, engine.ctx, int(first_step), int(nsteps), C.byref(idx)))
+        self.engines.append(engine)
+        return int(idx.value)
+
+    def set_shape(self, block=0, chunk_steps=0, blocks_per_sm=0, reg_cap=0):
+        sh = LimBatchShape(int(block), int(chunk_steps), int(blocks_per_sm), int(reg_cap))
+        self._check(self.lib.lim_batch_set_shape(self.h, C.byref(sh)))
+
+    def shape(self) -> dict:
+        sh = LimBatchShape()
+        self._check(self.lib.lim_batch_get_shape(self.h, C.byref(sh)))
+        return sh.as_dict()
+
+    def run(self):
+        self._check(self.lib.lim_batch_run(self.h))
+
+    def tune(self):
+        """Autotune the launch shape on this batch; returns (shape dict, best ms)."""
+        sh = LimBatchShape()
+        ms = C.c_double(0.0)
+        self._check(self.lib.lim_batch_tune(self.h, C.byref(sh), C.byref(ms)))
+        return sh.as_dict(), ms.value
+
+    def stats(self):
+        ms = C.c_double(0.0)
+        nl = C.c_int64(0)
+        ps = C.c_int64(0)
+        self._check(self.lib.lim_batch_stats(self.h, C.byref(ms), C.byref(nl), C.byref(ps)))
+        return ms.value, int(nl.value), int(ps.value)

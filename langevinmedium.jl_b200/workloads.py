@@ -14,6 +14,9 @@ medium from the same description.
   grid2p1     — 201×201 cells at 0.1 fm, 100 τ slices 0.6 → 10 fm/c, elliptic Gaussian
                 T0 = 0.45 GeV (σx 3.0, σy 2.4 fm) × (0.6/τ)^(1/3), radial flow
                 tanh(0.05 r (τ-0.6)), freeze-out latch at T < 0.155 GeV, Δt = 0.01.
+  batch       — 256 independent ensembles (counts log-uniform in [1e3, 1e6], charm or
+                bottom, 2πT·D_s ~ U[2,8], 500-2000 steps), half Bjorken, half 2+1D grids
+                with T0 ~ U[0.35,0.55] GeV and σy/σx ~ U[0.7,1.0].
 """
 from __future__ import annotations
 
@@ -58,6 +61,10 @@ def configure(eng: capi.Engine, wl: Workload, *, upload: bool = True):
         eng.set_medium_rt(med["xgrid"], med["tgrid"], med["T"], med["V"], med.get("V2"))
     elif med["kind"] == "bjorken":
         eng.set_medium_bjorken(med["T0"], med["tau0"], med["power"], med["r_max"])
+    elif med["kind"] == "grid_lazy":
+        g = grid2p1_fields(**med["args"])
+        eng.set_medium_grid(g["T"], g["ux"], g["uy"], g["x0"], g["dx"], g["y0"], g["dy"], g["tau0"], g["dtau"])
+        del g
     else:
         eng.set_medium_grid(med["T"], med["ux"], med["uy"], med["x0"], med["dx"], med["y0"], med["dy"],
                             med["tau0"], med["dtau"])
@@ -182,3 +189,63 @@ def grid2p1(N=5_000_000, *, m=1.5, precision="fp32", steps=None, seed=0x4C494D02
                   stop_after_freezeout=int(freezeout),
                   precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64, seed=seed)
     return Workload("grid2p1", params, med, spl, inv, x, p, 1, steps, dict(m=m))
+
+
+def grid2p1_lazy(**kw):
+    """A grid medium described by its generator arguments; ``configure`` builds the
+    fields when it loads the engine and drops them afterwards (the batch holds 128
+    grids of 64 MB each on the device, not on the host)."""
+    return dict(kind="grid_lazy", args=kw)
+
+
+def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3, 1e6), steps_range=(500, 2000),
+          grid_shape=(201, 201, 100), offset0=0):
+    """E independent ensembles for one batched launch: particle counts log-uniform in
+    n_range, masses from {1.5, 4.75} GeV, 2πT·D_s uniform in [2, 8], step counts uniform
+    in steps_range; half use the Bjorken medium (analytic T(τ), Δτ = 0.005), half 2+1D
+    grids with T0 uniform in [0.35, 0.55] GeV and σy/σx uniform in [0.7, 1.0] (σx = 3 fm,
+    Δt = 0.01).  Langevin + RTA, no freeze-out.  Particle ids are consecutive across
+    ensembles (particle_offset), so every ensemble has its own noise."""
+    rng = np.random.default_rng(rng_seed)
+    nx, ny, nt = grid_shape
+    kinds = np.array(["bjorken"] * (E // 2) + ["grid"] * (E - E // 2))
+    rng.shuffle(kinds)
+    lo, hi = math.log(n_range[0]), math.log(n_range[1])
+    invcdf_cache = {}
+    out = []
+    offset = int(offset0)
+    for e in range(E):
+        n = int(round(math.exp(rng.uniform(lo, hi))))
+        m = float(rng.choice([1.5, 4.75]))
+        DsT = float(rng.uniform(2.0, 8.0)) / TWO_PI
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        prec = capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64
+        if kinds[e] == "bjorken":
+            T0, tau0, dt = 0.40, 0.6, 0.005
+            med = dict(kind="bjorken", T0=T0, tau0=tau0, power=1.0 / 3.0, r_max=20.0)
+            Tmin, Tmax = T0 * (tau0 / (tau0 + (steps + 2) * dt)) ** (1.0 / 3.0), T0
+            x = rng.normal(0.0, 3.0, (2, n))
+            meta = dict(kind="bjorken", m=m)
+        else:
+            T0 = float(rng.uniform(0.35, 0.55))
+            sx = 3.0
+            sy = sx * float(rng.uniform(0.7, 1.0))
+            tau0, dt = 0.6, 0.01
+            med = grid2p1_lazy(nx=nx, ny=ny, nt=nt, T0=T0, sx=sx, sy=sy)
+            # the field's minimum: the grid corner at the last slice (grid2p1_fields)
+            xm, ym = (nx - 1) / 2 * 0.1, (ny - 1) / 2 * 0.1
+            Tmin = T0 * math.exp(-xm ** 2 / (2 * sx ** 2) - ym ** 2 / (2 * sy ** 2)) * (tau0 / 10.0) ** (1.0 / 3.0)
+            Tmax = T0
+            x = np.vstack([rng.normal(0.0, sx / math.sqrt(2), n), rng.normal(0.0, sy / math.sqrt(2), n)])
+            meta = dict(kind="grid", m=m, T0=T0, sx=sx, sy=sy)
+        p = rapidity_momenta(rng, n, m)
+        spl = {capi.LIM_SPLINE_DRAG: tr.build_tau_drag_spline(m, DsT, Tmin=Tmin, Tmax=Tmax, nT=1024),
+               capi.LIM_SPLINE_RTA: tr.build_tau_R_spline(m, DsT, eta_over_s=0.16, Tmin=Tmin, Tmax=Tmax, nT=1024)}
+        if m not in invcdf_cache:
+            invcdf_cache[m] = tr.build_juttner_invcdf(m, 3, Tmin=1e-3, Tmax=0.56)
+        params = dict(dt=dt, t0=tau0, m=m, DsT=DsT, dims=2, pdim=3, collision=capi.LIM_COLL_LANGEVIN_RTA,
+                      relativistic=1, bjorken_redshift=1, precision=prec, seed=seed, particle_offset=offset)
+        meta.update(DsT=DsT)
+        out.append(Workload(f"batch[{e}]", params, med, spl, invcdf_cache[m], x, p, 1, steps, meta))
+        offset += n
+    return out
