@@ -262,6 +262,8 @@ int block_of(const lim_ctx* c)
     return b;
 }
 
+constexpr int64_t kLiveSteps = 32;   // steps between compactions of the live list
+
 template <typename R>
 int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
              double* hist_x, double* hist_p)
@@ -276,6 +278,16 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
     if ((rc = dev_alloc(c, c->d_steps, (size_t)std::max<int64_t>(chunk_max, 1) * step_record_bytes<R>()))) return rc;
     kp.steps = c->d_steps.p;
     int64_t launches = 0;
+    // stop-at-freeze-out runs of the Cartesian kernels advance a compacted live list
+    const bool live_mode = c->P.coords == LIM_COORDS_CARTESIAN && kp.fo_capture && kp.stop_fo && kp.rec_steps == 0 &&
+                           c->n > 0 && c->n <= (int64_t)INT_MAX;
+    int cur = 0;
+    bool live_valid = false;
+    if (live_mode) {
+        if ((rc = dev_alloc(c, c->d_live[0], (size_t)c->n * sizeof(int)))) return rc;
+        if ((rc = dev_alloc(c, c->d_live[1], (size_t)c->n * sizeof(int)))) return rc;
+        if ((rc = dev_alloc(c, c->d_live_n, 2 * sizeof(unsigned)))) return rc;
+    }
     LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     int64_t s = first_step;
     while (s < end) {
@@ -286,8 +298,29 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
         }
         kp.step_base = s;
         kp.step_cap = chunk_end - s;
-        LIM_CUDA(c, launch_steps<R>(kp, (int)c->P.coords, s, chunk_end, block, c->stream));
-        launches += 2;                     // the per-step table, then the fused step kernel
+        if (!live_mode) {
+            LIM_CUDA(c, launch_steps<R>(kp, (int)c->P.coords, s, chunk_end, block, c->stream));
+            launches += 2;                 // the per-step table, then the fused step kernel
+        } else {
+            // Particles stop at freeze-out: advance the chunk in sub-chunks of kLiveSteps
+            // over a list of the live particles, compacted after each sub-chunk, so that
+            // the frozen ones do not idle the lanes of warps that still run.
+            LIM_CUDA(c, launch_step_table<R>(kp, 0, s, chunk_end, c->stream));
+            ++launches;
+            for (int64_t ss = s; ss < chunk_end; ss += kLiveSteps) {
+                const int64_t se = std::min<int64_t>(ss + kLiveSteps, chunk_end);
+                kp.live = live_valid ? (const int*)c->d_live[cur].p : nullptr;
+                kp.live_n = live_valid ? (const unsigned*)c->d_live_n.p + cur : nullptr;
+                LIM_CUDA(c, launch_steps_in_table<R>(kp, ss, se, block, c->stream));
+                LIM_CUDA(c, launch_compact_live(kp.fo_flag, kp.live, kp.live_n, c->n, (int*)c->d_live[cur ^ 1].p,
+                                                (unsigned*)c->d_live_n.p + (cur ^ 1), c->stream));
+                launches += 2;
+                cur ^= 1;
+                live_valid = true;
+            }
+            kp.live = nullptr;
+            kp.live_n = nullptr;
+        }
         const int64_t last = chunk_end - 1;
         if (saving && last % save_every == 0 && last >= 0) {
             const int64_t slot = last / save_every - first_slot;
@@ -514,7 +547,8 @@ int lim_destroy(lim_ctx* c)
     cudaStreamSynchronize(c->stream);
     DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
                       &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
-                      &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt };
+                      &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
+                      &c->d_live[0], &c->d_live[1], &c->d_live_n };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -541,7 +575,8 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
     if (!c || !bytes) return LIM_ERR_ARG;
     const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
                             &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
-                            &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt };
+                            &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
+                      &c->d_live[0], &c->d_live[1], &c->d_live_n };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)

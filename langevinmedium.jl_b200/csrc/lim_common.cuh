@@ -75,6 +75,9 @@ struct alignas(16) KParams {
     double* rec; int64_t rec_first, rec_steps;
     // per-step records (StepRec<R>, lim_step.cuh) for steps [step_base, step_base + step_cap)
     void* steps; int64_t step_base, step_cap;
+    // live list (runs that stop particles at freeze-out): when set, the step kernel
+    // advances only particles live[0 .. *live_n) (grid-stride), so that warps stay full
+    const int* live; const unsigned* live_n;
 };
 
 // ---------------------------------------------------------------------------

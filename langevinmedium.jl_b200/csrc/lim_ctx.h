@@ -52,6 +52,7 @@ struct lim_ctx {
     lim::DevBuf d_fo_pos[3], d_fo_mom[3], d_fo_tau, d_fo_flag, d_l_pos[3], d_l_mom[3], d_l_tau, d_l_T;
     lim::DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe, d_steps;
     lim::DevBuf d_rec, d_ckpt;
+    lim::DevBuf d_live[2], d_live_n;      // live lists of a stop-at-freeze-out run
     int64_t rec_first = 0, rec_steps = 0, ckpt_n = -1;
 
     // bumped by every call that may move or re-shape a device buffer, so that a batch

@@ -12,6 +12,16 @@ constexpr int kObsNum = 12;   // LIM_OBS_NUM
 template <typename R>
 cudaError_t launch_steps(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, int block, cudaStream_t st);
 
+// The per-step table alone (steps [s0, s1), s0 = kp.step_base), and Cartesian steps
+// [s0, s1) inside an already computed table (no table launch).
+template <typename R>
+cudaError_t launch_step_table(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, cudaStream_t st);
+template <typename R>
+cudaError_t launch_steps_in_table(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st);
+// Compacts the not-frozen particles of `in` (every index < n when in is NULL) into `out`.
+cudaError_t launch_compact_live(const double* flag, const int* in, const unsigned* in_n, int64_t n, int* out,
+                                unsigned* out_n, cudaStream_t st);
+
 // Bytes of one per-step record (the step table holds one per step of a launch).
 template <typename R>
 size_t step_record_bytes();

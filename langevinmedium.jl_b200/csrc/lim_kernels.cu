@@ -24,9 +24,44 @@ template <bool REC, bool FO, typename R, int MED, int DIMS, int PDIM>
 __global__ void __launch_bounds__(256)
 k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
 {
+    if (FO && kp.live) {                  // compacted list of the particles not yet frozen out
+        const unsigned cnt = *kp.live_n;
+        for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
+            cart_particle<REC, FO, R, MED, DIMS, PDIM>(kp, kp.rk, kp.live[k], s0, s1);
+        return;
+    }
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= kp.n) return;
     cart_particle<REC, FO, R, MED, DIMS, PDIM>(kp, kp.rk, i, s0, s1);
+}
+
+// Ordered-within-block compaction of the particles whose freeze-out flag is clear:
+// from `in` (or every index < n when in is NULL) to `out`; *out_n must be zero.
+__global__ void __launch_bounds__(256)
+k_compact_live(const double* __restrict__ flag, const int* __restrict__ in, const unsigned* in_n, int64_t n,
+               int* __restrict__ out, unsigned* out_n)
+{
+    __shared__ unsigned warp_cnt[8];
+    __shared__ unsigned base;
+    const unsigned cnt = in ? *in_n : (unsigned)n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (unsigned t0 = blockIdx.x * blockDim.x; t0 < cnt; t0 += gridDim.x * blockDim.x) {
+        const unsigned k = t0 + threadIdx.x;
+        int idx = -1;
+        if (k < cnt) idx = in ? in[k] : (int)k;
+        const bool keep = idx >= 0 && flag[idx] == 0.0;
+        const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) warp_cnt[warp] = __popc(ballot);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned tot = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { unsigned c = warp_cnt[w]; warp_cnt[w] = tot; tot += c; }
+            base = tot ? atomicAdd(out_n, tot) : 0u;
+        }
+        __syncthreads();
+        if (keep) out[base + warp_cnt[warp] + __popc(ballot & ((1u << lane) - 1u))] = idx;
+        __syncthreads();
+    }
 }
 
 template <bool REC, typename R>
@@ -77,7 +112,14 @@ static inline unsigned grid_of(int64_t n, int block) { return (unsigned)((n + bl
 template <bool REC, bool FO, typename R, int MED>
 static cudaError_t launch_cart_fo(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
 {
-    const unsigned g = grid_of(kp.n, block);
+    unsigned g = grid_of(kp.n, block);
+    if (FO && kp.live) {                  // grid-stride over the live list: a few waves of blocks
+        int sms = 0, dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const unsigned cap = (unsigned)sms * (unsigned)(2048 / block);
+        g = g < cap ? g : cap;
+    }
     const int dp = kp.dims * 10 + kp.pdim;
     if (MED == MED_GRID) {
         if (dp == 22) k_cart<REC, FO, R, MED, 2, 2><<<g, block, 0, st>>>(kp, s0, s1);
@@ -131,6 +173,51 @@ static cudaError_t launch_steps_rec(const KParams<R>& kp, int coords, int64_t s0
         return launch_cart_med<REC, R, MED_GRID>(kp, s0, s1, block, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// Steps [s0, s1) of a Cartesian run whose per-step table already holds them (no
+// table launch): the sub-chunks of a live-list run and of a checkpointed forward pass.
+template <typename R>
+cudaError_t launch_steps_in_table(const KParams<R>& kp, int64_t s0, int64_t s1, int block, cudaStream_t st)
+{
+    if (kp.n == 0 || s1 <= s0) return cudaSuccess;
+    if (!kp.steps || s0 < kp.step_base || s1 > kp.step_base + kp.step_cap) return cudaErrorInvalidValue;
+    switch (kp.med.kind) {
+    case MED_RT: return launch_cart_med<false, R, MED_RT>(kp, s0, s1, block, st);
+    case MED_BJORKEN: return launch_cart_med<false, R, MED_BJORKEN>(kp, s0, s1, block, st);
+    case MED_GRID: return launch_cart_med<false, R, MED_GRID>(kp, s0, s1, block, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <typename R>
+cudaError_t launch_step_table(const KParams<R>& kp, int coords, int64_t s0, int64_t s1, cudaStream_t st)
+{
+    if (s1 <= s0) return cudaSuccess;
+    if (!kp.steps || s0 != kp.step_base || s1 - s0 > kp.step_cap) return cudaErrorInvalidValue;
+    if (coords == 1) return launch_table<R, MED_MILNE_TABLE>(kp, s0, s1, st);
+    switch (kp.med.kind) {
+    case MED_RT: return launch_table<R, MED_RT>(kp, s0, s1, st);
+    case MED_BJORKEN: return launch_table<R, MED_BJORKEN>(kp, s0, s1, st);
+    case MED_GRID: return launch_table<R, MED_GRID>(kp, s0, s1, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_compact_live(const double* flag, const int* in, const unsigned* in_n, int64_t n, int* out,
+                                unsigned* out_n, cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(out_n, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    if (n <= 0) return cudaSuccess;
+    int sms = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    unsigned g = grid_of(n, 256);
+    const unsigned cap = (unsigned)sms * 8u;
+    g = g < cap ? g : cap;
+    k_compact_live<<<g, 256, 0, st>>>(flag, in, in_n, n, out, out_n);
+    return cudaGetLastError();
 }
 
 template <typename R>
@@ -355,6 +442,10 @@ size_t step_record_bytes() { return sizeof(StepRec<R>); }
 template size_t step_record_bytes<double>();
 template size_t step_record_bytes<float>();
 template cudaError_t launch_steps<double>(const KParams<double>&, int, int64_t, int64_t, int, cudaStream_t);
+template cudaError_t launch_steps_in_table<double>(const KParams<double>&, int64_t, int64_t, int, cudaStream_t);
+template cudaError_t launch_steps_in_table<float>(const KParams<float>&, int64_t, int64_t, int, cudaStream_t);
+template cudaError_t launch_step_table<double>(const KParams<double>&, int, int64_t, int64_t, cudaStream_t);
+template cudaError_t launch_step_table<float>(const KParams<float>&, int, int64_t, int64_t, cudaStream_t);
 template cudaError_t launch_steps<float>(const KParams<float>&, int, int64_t, int64_t, int, cudaStream_t);
 template cudaError_t launch_lab_boost<double>(const KParams<double>&, int, cudaStream_t);
 template cudaError_t launch_lab_boost<float>(const KParams<float>&, int, cudaStream_t);

@@ -178,11 +178,12 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     Local<R> L;
     L.nx = R(0); L.ny = R(0); L.v = R(0);
     if (MED == MED_GRID) {
+        // the grid holds the spatial four-velocity (u^x, u^y): speed |u| / sqrt(1 + u^2)
         R ux, uy;
         grid_lookup(kp.med, sr, x[0], x[1], L.T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
         L.boost = !(u < R(kEps));
-        L.v = u;
+        L.v = u / sqrt(fma(u, u, R(1)));
         if (L.boost) { L.nx = ux / u; L.ny = uy / u; }
     } else if (MED == MED_BJORKEN && fp32) {
         // zero flow: in FP32 the boost is the identity (gamma(0) rounds to 1)
@@ -213,12 +214,38 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     return L;
 }
 
-// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  The frame
-// change is evaluated in FP64 in both precisions: with the momentum held in FP64,
-// p_par - v E does not lose the LRF momentum to cancellation at large gamma.
+// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  FP64 path
+// and FP32 path at gamma >= 4: evaluated in FP64 (with the momentum held in FP64,
+// p_par - v E does not lose the LRF momentum to cancellation at large gamma).  FP32
+// path at gamma < 4: the FP32 increment (gamma - 1) p_par -/+ gamma v E along the flow
+// is added to the FP64 momentum; its error is ~eps gamma E.  Its operations are
+// explicitly rounded, so that every kernel inlining this step (plain, batched, taped)
+// computes the same bits whatever the compiler fuses around it.
 template <typename R, int DIMS, int PDIM>
 __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, double (&p)[3], bool to_lab)
 {
+    const float v2f = __fmul_rn((float)L.v, (float)L.v);
+    if (sizeof(R) == 4 && kp.rel && v2f < 0.9375f) {
+        const float vf = (float)L.v, mf = (float)kp.m;
+        const float g2 = 1.0f / __fsub_rn(1.0f, v2f);   // gamma^2; the 1e-10 is below FP32 resolution here
+        const float gam = sqrtf(g2);
+        const float gm1 = __fmul_rn(v2f, g2) / __fadd_rn(1.0f, gam);   // gamma - 1 without cancellation
+        float p2 = __fmul_rn(mf, mf);
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) { const float q = (float)p[d]; p2 = __fmaf_rn(q, q, p2); }
+        const float gvE = __fmul_rn(__fmul_rn(gam, vf), sqrtf(p2));
+        if (DIMS == 1) {
+            const float d = __fmaf_rn(gm1, (float)p[0], to_lab ? gvE : -gvE);
+            p[0] += (double)d;
+            return;
+        }
+        const float nxf = (float)L.nx, nyf = (float)L.ny;
+        const float ppar = __fmaf_rn((float)p[1], nyf, __fmul_rn((float)p[0], nxf));
+        const float d = __fmaf_rn(gm1, ppar, to_lab ? gvE : -gvE);
+        p[0] += (double)__fmul_rn(d, nxf);
+        p[1] += (double)__fmul_rn(d, nyf);
+        return;
+    }
     const double m = (double)kp.m;
     double v = (double)L.v;
     const double nx = (double)L.nx, ny = (double)L.ny;
@@ -410,7 +437,8 @@ __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int
     R nrm2 = R(0);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) nrm2 += g[d] * g[d];
-    R inv = pstar / sqrt(nrm2 > R(1e-300) ? nrm2 : R(1e-300));
+    const R tiny = (R)(sizeof(R) == 8 ? 1e-300 : 1e-30);   // the reference's 1e-300 guard, FP32-representable
+    R inv = pstar / sqrt(nrm2 > tiny ? nrm2 : tiny);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) p[d] = (double)(g[d] * inv);
 }
@@ -426,7 +454,8 @@ __device__ __forceinline__ void set_to_fluid(const KParams<R>& kp, const StepRec
         grid_lookup(kp.med, sr, x[0], x[1], T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
         if (u < R(kEps)) { p[0] = 0.0; p[1] = 0.0; return; }
-        R vc = kp.rel ? jclamp(u, -vmax, vmax) : u;
+        const R v = u / sqrt(fma(u, u, R(1)));          // four-velocity -> speed
+        R vc = kp.rel ? jclamp(v, -vmax, vmax) : v;
         R g = kp.rel ? R(1) / sqrt(R(1) - vc * vc + R(1e-10)) : R(1);
         p[0] = (double)(m * g * vc * (ux / u));
         p[1] = (double)(m * g * vc * (uy / u));
@@ -603,13 +632,9 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
 // Temperature at the particle in FP64 arithmetic (FP64 weights over the stored
 // field values), for the freeze-out latch of the FP32 path.
 template <typename R, int MED, int DIMS>
-__device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
-                                                   const float (&xl)[3])
+__device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const StepRec<R>& sr, const double (&xd)[3])
 {
     const MediumDev<R>& md = kp.med;
-    double xd[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (double)xl[d];
     double T;
     if (MED == MED_BJORKEN) {
         T = sr.Td;
@@ -660,14 +685,87 @@ __device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const S
     return T;
 }
 
+// The time record of medium time t (the FP64 fields make_step_rec derives from the
+// same t, so a temperature re-evaluated from it is bit-identical).
+template <typename R, int MED>
+__device__ __forceinline__ StepRec<R> step_rec_at_time(const KParams<R>& kp, double t)
+{
+    StepRec<R> u;
+    u.t = t; u.tR = (R)t; u.kt = 0; u.wt = R(0); u.T_bj = R(0); u.zf = 1.0; u.wtd = 0.0; u.Td = 0.0;
+    const MediumDev<R>& md = kp.med;
+    if (MED == MED_RT) {
+        const double* tg = md.tgd;
+        const int nt = md.nt;
+        double tq = t > tg[nt - 1] ? tg[nt - 1] : (t < tg[0] ? tg[0] : t);
+        int lo = -1, hi = nt;
+        while (hi - lo > 1) { int mid = (lo + hi) >> 1; if (tg[mid] <= tq) lo = mid; else hi = mid; }
+        int k = lo < 0 ? 0 : lo;
+        k = k > nt - 2 ? nt - 2 : k;
+        double y0 = tg[k], y1 = tg[k + 1], dy = y1 - y0;
+        u.kt = k;
+        u.wtd = fabs(dy) < kEps ? 0.0 : (tq - y0) / dy;
+    } else if (MED == MED_BJORKEN) {
+        u.Td = (t > md.bj_tau0) ? md.bj_T0 * pow(md.bj_tau0 / t, md.bj_power) : md.bj_T0;
+    } else {
+        double tq = t > md.gtl ? md.gtl : (t < md.gt0 ? md.gt0 : t);
+        double f = (tq - md.gt0) / md.gdt_d;
+        double fl = floor(f);
+        int it = fl < 0.0 ? 0 : (fl > (double)(md.gnt - 2) ? md.gnt - 2 : (int)fl);
+        u.kt = it;
+        u.wtd = f - (double)it;
+    }
+    return u;
+}
+
+// FP32 screen of the temperature at the particle: T in FP32 from the same nodes, off
+// from the FP64 value by far less than the latch's screening margin.
+template <typename R, int MED, int DIMS>
+__device__ __forceinline__ float temperature_screen(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3])
+{
+    const MediumDev<R>& md = kp.med;
+    if (MED == MED_BJORKEN) return (float)sr.T_bj * (float)md.T_scale;
+    if (MED == MED_GRID) {
+        int ix, iy;
+        R wx, wy;
+        grid_cell(md, x[0], x[1], ix, iy, wx, wy);
+        const float4* s0 = md.G + ((size_t)sr.kt * md.gny + iy) * md.gnx + ix;
+        const float4* s1 = s0 + (size_t)md.gny * md.gnx;
+        const float* q0 = reinterpret_cast<const float*>(s0);
+        const float* q1 = reinterpret_cast<const float*>(s1);
+        const int rowf = 4 * md.gnx;
+        const float fx = (float)wx, fy = (float)wy;
+        float a00 = __ldg(q0), a10 = __ldg(q0 + 4), a01 = __ldg(q0 + rowf), a11 = __ldg(q0 + rowf + 4);
+        float b00 = __ldg(q1), b10 = __ldg(q1 + 4), b01 = __ldg(q1 + rowf), b11 = __ldg(q1 + rowf + 4);
+        const float ra = a00 + fx * (a10 - a00), rb = b00 + fx * (b10 - b00);
+        const float c0 = ra + fy * ((a01 + fx * (a11 - a01)) - ra);
+        const float c1 = rb + fy * ((b01 + fx * (b11 - b01)) - rb);
+        return (c0 + (float)sr.wt * (c1 - c0)) * (float)md.T_scale;
+    }
+    R r;
+    if (DIMS == 1) r = fabs(x[0]);
+    else { R r2 = R(0);
+#pragma unroll
+        for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
+        r = sqrt(r2); }
+    return (float)temperature_at<R, MED, DIMS>(kp, sr, x, r);
+}
+
 // Freeze-out latch after streaming (kernels_gpu.jl:588-635), evaluated in FP64.
+// FP32 path: the FP64 temperature is evaluated only when an FP32 screen puts T
+// within kScreen of Tfo; a last-above step recorded from the screen alone keeps
+// lT = -1, and its FP64 temperature is re-evaluated from (lpos, ltau) when needed.
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
                                                 const R (&x)[3], const float (&xl)[3], const double (&p)[3],
                                                 double& flag, double (&lpos)[3], double (&lmom)[3],
                                                 double& ltau, double& lT)
 {
+    constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
     if (flag != 0.0) return;
+    double xd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (sizeof(R) == 4 ? (double)xl[d] : 0.0);
+    const double Tfo = (double)kp.Tfo;
     double T;
     if (sizeof(R) == 8) {
         R r;
@@ -678,12 +776,22 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
             r = sqrt(r2); }
         T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
     } else {
-        T = temperature_fp64<R, MED, DIMS>(kp, sr, x, xl);
-    }
-    double xd[3];
+        const float Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
+        if (Ts >= (float)Tfo + kScreen) {            // clearly above: remember the step only
 #pragma unroll
-    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (sizeof(R) == 4 ? (double)xl[d] : 0.0);
-    const double Tfo = (double)kp.Tfo;
+            for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
+            ltau = sr.t;
+            lT = -1.0;
+            return;
+        }
+        T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
+        if (T < Tfo && lT < 0.0) {
+            const StepRec<R> pr = step_rec_at_time<R, MED>(kp, ltau);
+            lT = temperature_fp64<R, MED, DIMS>(kp, pr, lpos);
+        }
+    }
     if (T < Tfo) {
         double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
 #pragma unroll

@@ -247,3 +247,17 @@ def test_observables_match_host_reduction(lmb):
     assert np.isclose(obs["mean_cos2phi"], np.mean((p[0] ** 2 - p[1] ** 2) / pt ** 2), rtol=1e-10)
     assert np.isclose(obs["frac_pt_gt"], np.mean(pt > 5.0), rtol=1e-12)
     assert np.isclose(obs["mean_p2"], np.mean(np.sum(p ** 2, axis=0)), rtol=1e-12)
+
+
+def test_live_list_run_matches_full_grid_run(lmb):
+    """Runs that stop particles at freeze-out advance a compacted list of the live
+    particles; the result equals the run over every particle (the noise-recording
+    instantiation takes that path), latch outputs included."""
+    for prec in ("fp32", "fp64"):
+        wl = build_case("grid_lrta_fo", prec, N=20000, steps=200)
+        a = engine_run(lmb, wl)
+        b = engine_run(lmb, wl, record=True)
+        assert 0.05 < np.mean(a["fo"]["flag"]) < 0.95
+        assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["p"], b["p"]), prec
+        for k in ("pos", "mom", "tau", "flag"):
+            assert np.array_equal(a["fo"][k], b["fo"][k]), (prec, k)
