@@ -60,7 +60,8 @@ enum {
     LIM_MEDIUM_BJORKEN = 1,     /* analytic T(tau) = T0 (tau0/tau)^p, zero transverse flow */
     LIM_MEDIUM_GRID    = 2      /* 2+1D grid T, u^x, u^y on (tau, x, y), trilinear */
 };
-enum { LIM_SPLINE_DRAG = 0, LIM_SPLINE_RTA = 1 };       /* transport.jl:208-222 */
+enum { LIM_SPLINE_DRAG = 0, LIM_SPLINE_RTA = 1,         /* transport.jl:208-222 */
+       LIM_SPLINE_DRAG_DA = 2, LIM_SPLINE_DRAG_DB = 3 }; /* d(drag time)/da, /db (lim_adjoint) */
 enum {                                                   /* observables reduced in FP64 on device */
     LIM_OBS_COUNT = 0,        /* number of particles counted (alive, or frozen-out when fo mode) */
     LIM_OBS_MEAN_PT,          /* <sqrt(px^2+py^2)> */
@@ -153,9 +154,25 @@ int lim_set_medium_grid(lim_ctx* ctx,
 
 /* Uniform-grid linear spline of a transport time in fm (transport.jl:165-253):
  * vals[k] at T = Tmin + k/invdT, k = 0..n-1.  which = LIM_SPLINE_DRAG (the drag
- * time 1/eta_D) or LIM_SPLINE_RTA (the RTA relaxation time). */
+ * time 1/eta_D) or LIM_SPLINE_RTA (the RTA relaxation time); LIM_SPLINE_DRAG_DA and
+ * LIM_SPLINE_DRAG_DB hold the derivatives of the drag values w.r.t. two parameters
+ * (a, b) of D_s(T) on the drag spline's grid, for lim_adjoint. */
 int lim_set_spline(lim_ctx* ctx, int which, double Tmin, double invdT,
                    const double* vals, int64_t n);
+
+/* Medium temperature scale s: every medium temperature is s * T (default 1).  No
+ * counterpart in the reference; the third parameter of lim_adjoint. */
+int lim_set_medium_scale(lim_ctx* ctx, double s);
+
+/* RTA decisions of steps [first_step, first_step + nsteps): mode 1 records the
+ * decisions of the following lim_run calls, mode 2 replays them (the collision
+ * indicator is taken from the record instead of comparing u_collide with dt/tau_R),
+ * mode 0 drops the record.  With the counter-based noise this fixes the whole random
+ * path of a run, as pathwise derivatives and their finite-difference checks need.  No
+ * counterpart in the reference.  lim_copy_rta_decisions copies a record between two
+ * contexts of the same particle count and sets the destination to replay. */
+int lim_rta_decisions(lim_ctx* ctx, int mode, int64_t first_step, int64_t nsteps);
+int lim_copy_rta_decisions(lim_ctx* dst, const lim_ctx* src);
 
 /* Jüttner inverse-CDF table (transport.jl:277-365): vals[jT*nU + iu] = p*(u_iu; T_jT). */
 int lim_set_invcdf(lim_ctx* ctx, const double* vals, int64_t nU, int64_t nT,
@@ -232,6 +249,25 @@ int lim_philox_device(lim_ctx* ctx, const uint32_t ctr[4], const uint32_t key[2]
 /* Device time of the last lim_run's step kernels in ms (CUDA events on the
  * context stream) and the number of kernel launches it issued. */
 int lim_last_run_stats(lim_ctx* ctx, double* kernel_ms, int64_t* launches);
+
+/* ---- pathwise gradients ----------------------------------------------------------
+ * lim_adjoint advances the state through steps [first_step, first_step + nsteps)
+ * exactly as lim_run does (checkpointing it every `checkpoint_every` steps, recording
+ * the RTA decisions), evaluates three final-state observables
+ *   obs[0] = <pT>, obs[1] = <cos 2 phi>, obs[2] = <sigmoid((pT - obs_pt_cut)/obs_pt_width)>
+ * and, with a hand-written reverse (adjoint) sweep that recomputes each segment from
+ * its checkpoint, their pathwise derivatives with the noise and the RTA indicators held
+ * fixed: grad[3*o + k] = d obs[o] / d theta_k for theta = (a, b, s), where a and b are
+ * the parameters of D_s(T) whose drag-spline derivatives were set with
+ * LIM_SPLINE_DRAG_DA / _DB and s is the medium scale (lim_set_medium_scale).  The
+ * run's RTA decisions stay recorded (replay mode) for finite-difference checks.
+ * Supported: FP32, Cartesian, dims 2, pdim 3, grid or analytic Bjorken medium,
+ * collision :langevin or :langevin_rta, relativistic, pre-point, no position
+ * diffusion, reflection or freeze-out.  No counterpart in the reference. */
+int lim_adjoint(lim_ctx* ctx, int64_t first_step, int64_t nsteps, int64_t checkpoint_every,
+                double* obs, double* grad);
+/* Device time (ms) of the last lim_adjoint: checkpointed forward and reverse sweep. */
+int lim_adjoint_stats(lim_ctx* ctx, double* forward_ms, double* reverse_ms);
 
 /* ---- batches ------------------------------------------------------------------
  * Many independent ensembles — each a configured context with its own particle

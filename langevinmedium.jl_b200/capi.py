@@ -22,7 +22,7 @@ LIM_OK, LIM_ERR_ARG, LIM_ERR_CUDA, LIM_ERR_STATE, LIM_ERR_NONFINITE, LIM_ERR_TIM
 LIM_FP64, LIM_FP32 = 0, 1
 LIM_COORDS_CARTESIAN, LIM_COORDS_MILNE = 0, 1
 LIM_COLL_LANGEVIN, LIM_COLL_RTA, LIM_COLL_LANGEVIN_RTA, LIM_COLL_FLUID = 0, 1, 2, 3
-LIM_SPLINE_DRAG, LIM_SPLINE_RTA = 0, 1
+LIM_SPLINE_DRAG, LIM_SPLINE_RTA, LIM_SPLINE_DRAG_DA, LIM_SPLINE_DRAG_DB = 0, 1, 2, 3
 LIM_NOISE_SLOTS = 11
 OBS_NAMES = ("count", "mean_pt", "mean_cos2phi", "frac_pt_gt", "frac_pt_gt_smooth", "mean_p2", "mean_E",
              "mean_lam1_num", "mean_px", "mean_wpx", "mean_pz2", "mean_x2")
@@ -91,6 +91,11 @@ _SIGS = {
     "lim_probe_fma_rate": ([C.c_void_p, _DP, _DP], C.c_int),
     "lim_observables_noalloc": ([C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_double,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
+    "lim_set_medium_scale": ([C.c_void_p, C.c_double], C.c_int),
+    "lim_rta_decisions": ([C.c_void_p, C.c_int, C.c_int64, C.c_int64], C.c_int),
+    "lim_copy_rta_decisions": ([C.c_void_p, C.c_void_p], C.c_int),
+    "lim_adjoint": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
+    "lim_adjoint_stats": ([C.c_void_p, _DP, _DP], C.c_int),
     "lim_batch_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "lim_batch_destroy": ([C.c_void_p], C.c_int),
     "lim_batch_last_error": ([C.c_void_p], C.c_char_p),
@@ -336,6 +341,32 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.lim_synchronize(self.ctx))
+
+    # -- pathwise gradients --------------------------------------------------------------
+    def set_medium_scale(self, s: float):
+        self._check(self.lib.lim_set_medium_scale(self.ctx, float(s)))
+
+    def rta_decisions(self, mode: int, first_step: int = 1, nsteps: int = 1):
+        """0 off, 1 record the following runs' RTA decisions, 2 replay them."""
+        self._check(self.lib.lim_rta_decisions(self.ctx, int(mode), int(first_step), int(nsteps)))
+
+    def copy_rta_decisions(self, src: "Engine"):
+        self._check(self.lib.lim_copy_rta_decisions(self.ctx, src.ctx))
+
+    def adjoint(self, first_step: int, nsteps: int, checkpoint_every: int = 64):
+        """Advance like run() and return (obs[3], grad[3, 3]): <pT>, <cos 2phi>, the smoothed
+        fraction above obs_pt_cut, and their derivatives w.r.t. (a, b, s)."""
+        obs = np.zeros(3)
+        grad = np.zeros(9)
+        self._check(self.lib.lim_adjoint(self.ctx, int(first_step), int(nsteps), int(checkpoint_every),
+                                         _dptr(obs), _dptr(grad)))
+        return obs, grad.reshape(3, 3)
+
+    def adjoint_stats(self):
+        f = C.c_double(0.0)
+        r = C.c_double(0.0)
+        self._check(self.lib.lim_adjoint_stats(self.ctx, C.byref(f), C.byref(r)))
+        return f.value, r.value
 
 
 class Batch:

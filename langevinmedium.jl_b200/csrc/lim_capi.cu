@@ -133,7 +133,7 @@ int ensure_device_medium(lim_ctx* c)
         for (size_t k = 0; k < nn; ++k) g[k] = make_float4(c->gT[k], c->gux[k], c->guy[k], 0.f);
         if ((rc = upload(c, c->d_G, g.data(), nn))) return rc;
     }
-    for (int w = 0; w < 2; ++w) {
+    for (int w = 0; w < 4; ++w) {
         if (c->spl[w].empty()) continue;
         std::vector<R> s(c->spl[w].size());
         for (size_t k = 0; k < s.size(); ++k) s[k] = (R)c->spl[w][k];
@@ -189,6 +189,12 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
         }
     }
     kp.spl_shared = kp.n_drag == kp.n_rta && kp.drag_Tmin == kp.rta_Tmin && kp.drag_invdT == kp.rta_invdT;
+    kp.drag_da = c->spl[2].empty() ? nullptr : (const R*)c->d_spl[2].p;
+    kp.drag_db = c->spl[3].empty() ? nullptr : (const R*)c->d_spl[3].p;
+    kp.rta_bits = (uint32_t*)c->d_rta_bits.p;
+    kp.rta_mode = c->d_rta_bits.p ? c->rta_mode : 0;
+    kp.rta_first = c->rta_first;
+    kp.rta_steps = c->rta_steps;
     kp.icdf = (const R*)c->d_icdf.p; kp.nU = (int)c->nU; kp.nT = (int)c->nT;
     kp.ic_Tmin = (R)c->ic_Tmin; kp.ic_invdT = (R)c->ic_invdT;
     MediumDev<R>& md = kp.med;
@@ -500,6 +506,7 @@ int ctx_fail(lim_ctx* c, int code, const char* fmt, ...)
     return fail(c, code, "%s", buf);
 }
 int ctx_check_ready(lim_ctx* c) { return check_ready(c); }
+int ctx_alloc(lim_ctx* c, DevBuf& b, size_t bytes) { return dev_alloc(c, b, bytes); }
 template <typename R> int ctx_build_kparams(lim_ctx* c, KParams<R>& kp) { return build_kparams<R>(c, kp); }
 template int ctx_build_kparams<double>(lim_ctx*, KParams<double>&);
 template int ctx_build_kparams<float>(lim_ctx*, KParams<float>&);
@@ -545,10 +552,12 @@ int lim_destroy(lim_ctx* c)
     if (!c) return LIM_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
                       &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
                       &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
-                      &c->d_live[0], &c->d_live[1], &c->d_live_n };
+                      &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
+                      &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -573,10 +582,12 @@ int lim_synchronize(lim_ctx* c)
 int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
 {
     if (!c || !bytes) return LIM_ERR_ARG;
-    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_icdf,
+    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
                             &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
                             &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
-                      &c->d_live[0], &c->d_live[1], &c->d_live_n };
+                      &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
+                      &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -687,13 +698,61 @@ int lim_set_spline(lim_ctx* c, int which, double Tmin, double invdT, const doubl
 {
     if (!c) return LIM_ERR_ARG;
     ++c->gen;
-    if (which != LIM_SPLINE_DRAG && which != LIM_SPLINE_RTA) return fail(c, LIM_ERR_ARG, "lim_set_spline: unknown spline %d", which);
+    if (which < LIM_SPLINE_DRAG || which > LIM_SPLINE_DRAG_DB) return fail(c, LIM_ERR_ARG, "lim_set_spline: unknown spline %d", which);
     if (!vals || n < 1) return fail(c, LIM_ERR_ARG, "lim_set_spline: empty spline");
     if (!std::isfinite(Tmin) || !std::isfinite(invdT)) return fail(c, LIM_ERR_ARG, "lim_set_spline: non-finite Tmin/invdT");
     c->spl[which].assign(vals, vals + n);
     c->spl_Tmin[which] = Tmin;
     c->spl_invdT[which] = invdT;
     c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_set_medium_scale(lim_ctx* c, double s)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!std::isfinite(s) || !(s > 0)) return fail(c, LIM_ERR_ARG, "lim_set_medium_scale: scale must be finite and > 0");
+    ++c->gen;
+    c->T_scale = s;
+    return LIM_OK;
+}
+
+int lim_rta_decisions(lim_ctx* c, int mode, int64_t first_step, int64_t nsteps)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (mode < 0 || mode > 2) return fail(c, LIM_ERR_ARG, "lim_rta_decisions: mode must be 0 (off), 1 (record) or 2 (replay)");
+    ++c->gen;
+    if (mode == 0) { dev_free(c->d_rta_bits); c->rta_mode = 0; c->rta_steps = 0; return LIM_OK; }
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "upload the state before recording or replaying RTA decisions");
+    if (first_step < 0 || nsteps < 1) return fail(c, LIM_ERR_ARG, "lim_rta_decisions: need first_step >= 0 and nsteps >= 1");
+    const size_t words = (size_t)((nsteps + 31) / 32) * (size_t)c->n;
+    if (mode == 1) {
+        int rc = dev_alloc(c, c->d_rta_bits, std::max<size_t>(words, 1) * sizeof(uint32_t));
+        if (rc) return rc;
+        LIM_CUDA(c, cudaMemsetAsync(c->d_rta_bits.p, 0, std::max<size_t>(words, 1) * sizeof(uint32_t), c->stream));
+        c->rta_first = first_step;
+        c->rta_steps = nsteps;
+    } else {
+        if (!c->d_rta_bits.p || c->rta_first != first_step || c->rta_steps != nsteps || c->d_rta_bits.bytes < words * sizeof(uint32_t))
+            return fail(c, LIM_ERR_STATE, "lim_rta_decisions: replay needs decisions recorded for the same steps and particles");
+    }
+    c->rta_mode = mode;
+    return LIM_OK;
+}
+
+int lim_copy_rta_decisions(lim_ctx* dst, const lim_ctx* src)
+{
+    if (!dst || !src) return LIM_ERR_ARG;
+    if (!src->d_rta_bits.p || src->n != dst->n)
+        return fail(dst, LIM_ERR_STATE, "lim_copy_rta_decisions: the source holds no decisions for this particle count");
+    ++dst->gen;
+    int rc = dev_alloc(dst, dst->d_rta_bits, src->d_rta_bits.bytes);
+    if (rc) return rc;
+    LIM_CUDA(dst, cudaStreamSynchronize(src->stream));
+    LIM_CUDA(dst, cudaMemcpyAsync(dst->d_rta_bits.p, src->d_rta_bits.p, src->d_rta_bits.bytes, cudaMemcpyDeviceToDevice, dst->stream));
+    dst->rta_first = src->rta_first;
+    dst->rta_steps = src->rta_steps;
+    dst->rta_mode = 2;
     return LIM_OK;
 }
 

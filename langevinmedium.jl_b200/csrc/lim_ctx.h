@@ -32,8 +32,8 @@ struct lim_ctx {
     int64_t gnx = 0, gny = 0, gnt = 0;
     double gx0 = 0, gdx = 0, gy0 = 0, gdy = 0, gt0 = 0, gdt = 0;
     std::vector<float> gT, gux, guy;
-    std::vector<double> spl[2];
-    double spl_Tmin[2] = { 0, 0 }, spl_invdT[2] = { 1, 1 };
+    std::vector<double> spl[4];           // drag, RTA, d(drag)/da, d(drag)/db
+    double spl_Tmin[4] = { 0, 0, 0, 0 }, spl_invdT[4] = { 1, 1, 1, 1 };
     std::vector<double> icdf;
     int64_t nU = 0, nT = 0;
     double ic_Tmin = 0, ic_invdT = 1;
@@ -42,7 +42,7 @@ struct lim_ctx {
     // device copy of the medium for `dev_prec`
     int dev_prec = -1;
     bool dev_dirty = true;
-    lim::DevBuf d_xg, d_tg, d_tgd, d_xgd, d_TV, d_V2, d_G, d_spl[2], d_icdf;
+    lim::DevBuf d_xg, d_tg, d_tgd, d_xgd, d_TV, d_V2, d_G, d_spl[4], d_icdf;
 
     // particle state (structure of arrays, precision `state_prec`)
     int64_t n = 0;
@@ -53,6 +53,12 @@ struct lim_ctx {
     lim::DevBuf d_status, d_stage_x, d_stage_p, d_partials, d_obs, d_probe, d_steps;
     lim::DevBuf d_rec, d_ckpt;
     lim::DevBuf d_live[2], d_live_n;      // live lists of a stop-at-freeze-out run
+    lim::DevBuf d_rta_bits;               // recorded / replayed RTA decisions
+    int rta_mode = 0;
+    int64_t rta_first = 0, rta_steps = 0;
+    lim::DevBuf d_adj_ckpt, d_adj_tape, d_adj_table, d_adj_part, d_adj_out;   // lim_adjoint
+    lim::DevBuf d_adj_lam, d_adj_gacc, d_adj_slope, d_adj_icdt;
+    double adj_fwd_ms = 0.0, adj_rev_ms = 0.0;
     int64_t rec_first = 0, rec_steps = 0, ckpt_n = -1;
 
     // bumped by every call that may move or re-shape a device buffer, so that a batch
@@ -69,6 +75,7 @@ namespace lim {
 
 // Context services used by the batch entry points (defined in lim_capi.cu).
 int ctx_fail(lim_ctx* c, int code, const char* fmt, ...);
+int ctx_alloc(lim_ctx* c, DevBuf& b, size_t bytes);
 int ctx_check_ready(lim_ctx* c);
 template <typename R> int ctx_build_kparams(lim_ctx* c, KParams<R>& kp);
 

@@ -63,6 +63,24 @@ cudaError_t batch_blocks_per_sm(int dims, int pdim, bool fo, bool cap, int block
 template <typename R>
 cudaError_t launch_batch_table(const KParams<R>& kp, int64_t s0, int64_t n, void* out, cudaStream_t st);
 
+// Reverse sweep of lim_adjoint (lim_adjoint.cu).  Checkpoint k of the forward pass,
+// at byte offset k * (segment bytes): x[2] (float), x_lo[2] (float), p[3] (double),
+// each n long.  The tape (KParams::tape) holds kTapeFields floats per particle per
+// step of one segment; lam the 2 x 5 cotangents, gacc the 2 x 3 parameter sums.
+constexpr int kAdjOut = 12;      // 3 observables + 3 x 3 gradients
+constexpr int kAdjCot = 2;       // cotangents: the final p_x and p_y
+constexpr int kAdjBlock = 128;
+struct AdjointArgs {
+    float* lam;
+    double* gacc;
+    double cut, width;
+    double* partials;            // [nblocks][kAdjOut]
+};
+cudaError_t launch_adjoint_seed(const KParams<float>& kp, const AdjointArgs& aa, cudaStream_t st);
+cudaError_t launch_adjoint_tape(const KParams<float>& kp, int64_t s0, int64_t s1, cudaStream_t st);
+cudaError_t launch_adjoint_rev(const KParams<float>& kp, const AdjointArgs& aa, int64_t s0, int64_t s1, cudaStream_t st);
+cudaError_t launch_adjoint_total(const KParams<float>& kp, const AdjointArgs& aa, double* out, cudaStream_t st);
+
 cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
 
 // FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.

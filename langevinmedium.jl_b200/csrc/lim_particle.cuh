@@ -46,7 +46,7 @@ __device__ __forceinline__ bool state_finite(const R (&x)[3], const double (&p)[
 
 // Steps [s0, s1) of particle i.  rk: the Philox round keys (kernel-parameter
 // constants in both kernels); kp: the ensemble's parameters.
-template <bool REC, bool FO, typename R, int MED, int DIMS, int PDIM>
+template <int REC, bool FO, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2* __restrict__ rk, int64_t i,
                                               int64_t s0, int64_t s1)
 {
@@ -68,6 +68,11 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && flag != 0.0) break;
         const StepRec<R> sr = tab[s];
+        if (REC == 2) {                   // the adjoint's tape: the pre-step state
+            float* t = kp.tape + (s - kp.tape_first) * kTapeFields * kp.n + i;
+            t[0] = (float)x[0]; t[kp.n] = (float)x[1];
+            t[2 * kp.n] = (float)p[0]; t[3 * kp.n] = (float)p[1]; t[4 * kp.n] = (float)p[2];
+        }
         cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
         if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT);
         if (!state_finite<R, DIMS, PDIM>(x, p)) {

@@ -214,38 +214,14 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     return L;
 }
 
-// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  FP64 path
-// and FP32 path at gamma >= 4: evaluated in FP64 (with the momentum held in FP64,
-// p_par - v E does not lose the LRF momentum to cancellation at large gamma).  FP32
-// path at gamma < 4: the FP32 increment (gamma - 1) p_par -/+ gamma v E along the flow
-// is added to the FP64 momentum; its error is ~eps gamma E.  Its operations are
-// explicitly rounded, so that every kernel inlining this step (plain, batched, taped)
-// computes the same bits whatever the compiler fuses around it.
+// kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  The frame
+// change is evaluated in FP64 in both precisions: with the momentum held in FP64,
+// p_par - v E does not lose the LRF momentum to cancellation at large gamma, and no
+// FP32 rounding of the momentum enters the state (FP32 increments of the frame change
+// cost up to 1e-5 of relative error over a few hundred steps at gamma ~ 1.4).
 template <typename R, int DIMS, int PDIM>
 __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, double (&p)[3], bool to_lab)
 {
-    const float v2f = __fmul_rn((float)L.v, (float)L.v);
-    if (sizeof(R) == 4 && kp.rel && v2f < 0.9375f) {
-        const float vf = (float)L.v, mf = (float)kp.m;
-        const float g2 = 1.0f / __fsub_rn(1.0f, v2f);   // gamma^2; the 1e-10 is below FP32 resolution here
-        const float gam = sqrtf(g2);
-        const float gm1 = __fmul_rn(v2f, g2) / __fadd_rn(1.0f, gam);   // gamma - 1 without cancellation
-        float p2 = __fmul_rn(mf, mf);
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) { const float q = (float)p[d]; p2 = __fmaf_rn(q, q, p2); }
-        const float gvE = __fmul_rn(__fmul_rn(gam, vf), sqrtf(p2));
-        if (DIMS == 1) {
-            const float d = __fmaf_rn(gm1, (float)p[0], to_lab ? gvE : -gvE);
-            p[0] += (double)d;
-            return;
-        }
-        const float nxf = (float)L.nx, nyf = (float)L.ny;
-        const float ppar = __fmaf_rn((float)p[1], nyf, __fmul_rn((float)p[0], nxf));
-        const float d = __fmaf_rn(gm1, ppar, to_lab ? gvE : -gvE);
-        p[0] += (double)__fmul_rn(d, nxf);
-        p[1] += (double)__fmul_rn(d, nyf);
-        return;
-    }
     const double m = (double)kp.m;
     double v = (double)L.v;
     const double nx = (double)L.nx, ny = (double)L.ny;
@@ -277,12 +253,15 @@ __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, d
     p[1] = pnew * ny + pperpy;
 }
 
-// Records a consumed variate (noise-recording instantiation only).
-template <bool REC, typename R>
+// Records a consumed variate.  REC = 1: the noise-recording instantiation (every
+// slot, FP64); REC = 2: the adjoint's tape (the momentum normals, FP32).
+template <int REC, typename R>
 __device__ __forceinline__ void rec_slot(const KParams<R>& kp, int64_t s, int64_t i, int slot, double val)
 {
-    if (REC && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
+    if (REC == 1 && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
         kp.rec[((s - kp.rec_first) * kNoiseSlots + slot) * kp.n + i] = (double)val;
+    if (REC == 2 && slot < 3)
+        kp.tape[((s - kp.tape_first) * kTapeFields + 5 + slot) * kp.n + i] = (float)val;
 }
 
 // expm1(-x) for x >= 0: Taylor series below 0.05 (truncation < 1e-11 relative),
@@ -414,12 +393,19 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, uint32_t w, R T
 // uniform u_collide comes with the step's momentum variates; the sample and the
 // direction are drawn only when the particle collides.
 // tn: the RTA relaxation time (0 when DsT <= 0 or T <= 0), kernels_gpu.jl:675-679.
-template <bool REC, typename R, int DIMS, int PDIM>
+template <int REC, typename R, int DIMS, int PDIM>
 __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, const NoiseKey& nk,
                                             R T, R tn, R uc, double (&p)[3])
 {
     R Pcol = (tn > R(0) && isfinite(tn)) ? jclamp(kp.dtR / tn, R(0), R(1)) : R(1);
-    if (!(uc < Pcol || Pcol >= R(1))) return;
+    bool collide = uc < Pcol || Pcol >= R(1);
+    if (kp.rta_mode && s >= kp.rta_first && s < kp.rta_first + kp.rta_steps) {
+        uint32_t* w = kp.rta_bits + ((s - kp.rta_first) >> 5) * kp.n + i;
+        const uint32_t bit = 1u << ((s - kp.rta_first) & 31);
+        if (kp.rta_mode == 2) collide = (*w & bit) != 0u;
+        else if (collide) *w |= bit;
+    }
+    if (!collide) return;
     const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTA);
     R pstar = invcdf_lookup(kp, u.x, T);
     R g[3];
@@ -503,7 +489,7 @@ __device__ __forceinline__ void acc_add(R& hi, float& lo, R dx)
 }
 
 // kernels_cpu.jl:510-637
-template <bool REC, typename R, int MED, int DIMS, int PDIM>
+template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                                  const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
@@ -585,7 +571,7 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
 }
 
 // One Cartesian step (simulate_cpu.jl:215-290).
-template <bool REC, typename R, int MED, int DIMS, int PDIM>
+template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
@@ -833,7 +819,7 @@ __device__ __forceinline__ void milne_lookup(const MediumDev<R>& md, const StepR
     V = c0 * (R(1) - yd) + c1 * yd;
 }
 
-template <bool REC, typename R>
+template <int REC, typename R>
 __device__ __forceinline__ void milne_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                            const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {

@@ -138,6 +138,27 @@ def build_tau_R_spline(m, DsT, *, eta_over_s=0.16, factor=5.0, **kw):
     return _build_time_spline(fn, m, DsT, **kw)
 
 
+def ds_linear_params(a, b, Tc=0.155):
+    """2πT·D_s = a + b (max(T, Tc)/Tc - 1): the reference's linear D_s form
+    (effective_DsT with DsT_linear, transport.jl:139-156) with Tfo = Tc,
+    DsT_slope = b/(2π Tc) and DsT_offset = (a - b)/(2π)."""
+    two_pi = 2.0 * math.pi
+    return dict(DsT_linear=True, DsT_slope=float(b) / (two_pi * Tc), DsT_offset=(float(a) - float(b)) / two_pi,
+                Tfo=float(Tc))
+
+
+def build_drag_spline_ab(m, a, b, *, Tc=0.155, Tmin, Tmax, nT=1024):
+    """Drag-time spline for 2πT·D_s = a + b (max(T, Tc)/Tc - 1) and its exact derivatives
+    with respect to a and b on the same grid (tau_drag = m D_s T / T^2, transport.jl:132-137):
+    returns (Tmin, invdT, vals, d_da, d_db)."""
+    Tm, inv, vals = build_tau_drag_spline(m, 1.0, Tmin=Tmin, Tmax=Tmax, nT=nT, **ds_linear_params(a, b, Tc))
+    T = Tm + np.arange(len(vals)) / inv
+    base = float(m) / (T * T) / fmGeV / (2.0 * math.pi) * LV_TAUN_SCALE
+    d_da = base.copy()
+    d_db = base * (np.maximum(T, Tc) / Tc - 1.0)
+    return Tm, inv, vals, d_da, d_db
+
+
 def eval_tau_n_spline(T, Tmin, invdT, tau_vals) -> float:
     """transport.jl:231-253 (scalar)."""
     n = len(tau_vals)

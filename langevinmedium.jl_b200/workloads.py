@@ -15,6 +15,8 @@ medium from the same description.
                 T0 = 0.45 GeV (σx 3.0, σy 2.4 fm) × (0.6/τ)^(1/3), radial four-velocity
                 u^r = tanh(0.05 r (τ-0.6)) (fields hold u^x, u^y; speed u/sqrt(1+u²)),
                 freeze-out latch at T < 0.155 GeV, Δt = 0.01.
+  adjoint_grid — the grid medium for pathwise gradients: 1e6 charm, 2000 steps, no
+                freeze-out, 2πT·D_s = a + b (T/0.155 - 1) and a temperature scale s.
   batch       — 256 independent ensembles (counts log-uniform in [1e3, 1e6], charm or
                 bottom, 2πT·D_s ~ U[2,8], 500-2000 steps), half Bjorken, half 2+1D grids
                 with T0 ~ U[0.35,0.55] GeV and σy/σx ~ U[0.7,1.0].
@@ -73,6 +75,8 @@ def configure(eng: capi.Engine, wl: Workload, *, upload: bool = True):
         eng.set_spline(which, a, b, v)
     if wl.invcdf is not None:
         eng.set_invcdf(*wl.invcdf)
+    if wl.meta.get("scale", 1.0) != 1.0:
+        eng.set_medium_scale(wl.meta["scale"])
     if upload:
         eng.upload_state(wl.x, wl.p)
 
@@ -250,3 +254,26 @@ def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3,
         out.append(Workload(f"batch[{e}]", params, med, spl, invcdf_cache[m], x, p, 1, steps, meta))
         offset += n
     return out
+
+
+def adjoint_grid(N=1_000_000, *, a=3.0, b=2.0, scale=1.0, steps=2000, m=1.5, precision="fp32",
+                 seed=0x4C494D03, rng_seed=5, dt=0.01, fields=None, eta_over_s=0.16, pt_cut=5.0, pt_width=0.1):
+    """Differentiation workload: the 2+1D grid medium, charm, Langevin + RTA, no freeze-out,
+    2πT·D_s = a + b (max(T, 0.155)/0.155 - 1), medium temperature scale s.  The drag
+    spline comes with its derivative tables in (a, b) for lim_adjoint."""
+    med = fields or grid2p1_fields()
+    tau0 = med["tau0"]
+    rng = np.random.default_rng(rng_seed)
+    sx, sy = 3.0, 2.4
+    x = np.vstack([rng.normal(0.0, sx / math.sqrt(2), N), rng.normal(0.0, sy / math.sqrt(2), N)])
+    p = rapidity_momenta(rng, N, m)
+    Tmin, Tmax = tr.spline_range(med["T"])
+    Tm, inv, vals, d_da, d_db = tr.build_drag_spline_ab(m, a, b, Tmin=Tmin, Tmax=Tmax, nT=1024)
+    spl = {capi.LIM_SPLINE_DRAG: (Tm, inv, vals), capi.LIM_SPLINE_DRAG_DA: (Tm, inv, d_da),
+           capi.LIM_SPLINE_DRAG_DB: (Tm, inv, d_db),
+           capi.LIM_SPLINE_RTA: tr.build_tau_R_spline(m, 1.0, eta_over_s=eta_over_s, Tmin=Tmin, Tmax=Tmax, nT=1024)}
+    inv_cdf = tr.build_juttner_invcdf(m, 3, Tmin=Tmin, Tmax=Tmax)
+    params = dict(dt=dt, t0=tau0, m=m, DsT=a / TWO_PI, dims=2, pdim=3, collision=capi.LIM_COLL_LANGEVIN_RTA,
+                  relativistic=1, bjorken_redshift=1, obs_pt_cut=pt_cut, obs_pt_width=pt_width,
+                  precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64, seed=seed)
+    return Workload("adjoint_grid", params, med, spl, inv_cdf, x, p, 1, steps, dict(m=m, a=a, b=b, scale=scale))

@@ -41,6 +41,10 @@ typedef struct orc_params {
             position_diffusion, reflecting_boundary, integrator_mode,
             freezeout_capture, freezeout_interp, precision, seed,
             particle_offset, stop_after_freezeout, block_size;
+    /* with recorded noise: 1 takes the RTA decisions from the record (a particle
+     * collided at a step iff its u_sample slot is non-zero) instead of uc < Pcol,
+     * which holds the RTA indicators fixed under parameter changes */
+    int64_t rta_replay;
 } orc_params;
 
 typedef struct orc_medium {
@@ -549,7 +553,9 @@ static void rta_collide(const orc_params* P, const orc_medium* md, const noise_s
     double tn = (P->DsT > 0.0 && T > 0.0) ? eval_spline(T, md->rta_Tmin, md->rta_invdT, md->rta, md->n_rta) : 0.0;
     double Pcol = (tn > 0.0 && jl_isfinite(tn)) ? jl_clamp(P->dt / tn, 0.0, 1.0) : 1.0;
     /* rand() < Pcol with rand() in [0,1): Pcol = 1 always collides */
-    if (!(uc < Pcol || Pcol >= 1.0)) return;
+    int collide = uc < Pcol || Pcol >= 1.0;
+    if (P->rta_replay && ns->rec) collide = rec_at(ns, i, step, 4) != 0.0;
+    if (!collide) return;
     double us, g[3];
     draw_rta_sample(P, ns, i, step, &us, g);
     double pstar = invcdf_lookup(md, us, T);

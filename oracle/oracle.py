@@ -24,7 +24,7 @@ class OrcParams(C.Structure):
                [(n, C.c_int64) for n in ("dims", "pdim", "coords", "collision", "relativistic", "bjorken_redshift",
                                          "position_diffusion", "reflecting_boundary", "integrator_mode",
                                          "freezeout_capture", "freezeout_interp", "precision", "seed",
-                                         "particle_offset", "stop_after_freezeout", "block_size")]
+                                         "particle_offset", "stop_after_freezeout", "block_size", "rta_replay")]
 
 
 _DP = C.POINTER(C.c_double)
@@ -99,7 +99,7 @@ def make_params(**kw) -> OrcParams:
     d = dict(dt=0.001, t0=0.0, m=1.0, DsT=0.2, Tfo=0.156, psi2=0.0, obs_pt_cut=5.0, obs_pt_width=0.1, dims=3, pdim=0,
              coords=0, collision=0, relativistic=1, bjorken_redshift=0, position_diffusion=0, reflecting_boundary=0,
              integrator_mode=0, freezeout_capture=0, freezeout_interp=1, precision=0, seed=0x4C494D00,
-             particle_offset=0, stop_after_freezeout=0, block_size=0)
+             particle_offset=0, stop_after_freezeout=0, block_size=0, rta_replay=0)
     d.update(kw)
     if d["pdim"] <= 0:
         d["pdim"] = d["dims"]
@@ -151,8 +151,9 @@ class Medium:
         v = self._k(vals)
         if which == 0:
             self.s.drag, self.s.n_drag, self.s.drag_Tmin, self.s.drag_invdT = _d(v), v.size, Tmin, invdT
-        else:
+        elif which == 1:
             self.s.rta, self.s.n_rta, self.s.rta_Tmin, self.s.rta_invdT = _d(v), v.size, Tmin, invdT
+        # the drag-derivative tables (2, 3) belong to the engine's reverse sweep only
         return self
 
     def invcdf(self, vals, nU, nT, Tmin, invdT):

@@ -135,6 +135,8 @@ def oracle_medium(orc, wl):
         md.spline(w, a, b, v)
     if wl.invcdf is not None:
         md.invcdf(*wl.invcdf)
+    if wl.meta.get("scale", 1.0) != 1.0:
+        md.scale(wl.meta["scale"])
     return md
 
 
