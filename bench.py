@@ -11,6 +11,9 @@ redshift, FP32 arithmetic with FP64 momentum accumulation.  Synthetic seeded inp
           device checkpoint before every pass); L2 flushed between passes.
   e2e   : the same through the C-ABI from pinned host buffers: upload, step-0 boost,
           run, download of the final state, every pass.
+  batched / adjoint / grid2p1 (one-GPU run): the batched persistent launch of 256
+          ensembles against 256 separate runs, the forward+adjoint cost against the
+          plain forward, and the 2+1D grid workload with freeze-out and its roofline.
 
 `--impl reference` times the reference's CPU algorithm (the FP64 restatement under
 oracle/, all host threads) on a bounded sample of the same workload.
@@ -185,6 +188,174 @@ def traffic_from_profile():
     return None
 
 
+# ---------------------------------------------------------------------------------
+# the other two legs of the metric (measured at N = 1): batched vs separate launches,
+# and the forward+adjoint cost; plus the 2+1D grid workload's roofline
+# ---------------------------------------------------------------------------------
+TUNED = ROOT / "langevinmedium.jl_b200" / "tuned_shapes.json"
+
+
+def bench_batched(pkg, args, flush):
+    """256 ensembles (1e3-1e6 particles, charm/bottom, 2piT Ds in [2, 8], 500-2000 steps,
+    half Bjorken, half 2+1D grids): one batched run (graph of persistent chunk launches)
+    against the same ensembles as 256 lim_run calls back to back."""
+    import torch
+    W, capi = pkg.workloads, pkg.capi
+    wls = W.batch(E=256)
+    engs = []
+    for wl in wls:
+        e = capi.Engine(0)
+        W.configure(e, wl)
+        e.initial_lab_boost()
+        e.state_save()
+        engs.append(e)
+    ps = sum(w.n * w.steps for w in wls)
+    reps = max(1, min(args.steps, 3))
+
+    def restore():
+        for e in engs:
+            e.state_restore()
+        for e in engs:
+            e.synchronize()
+
+    sep_wall, sep_dev = [], []
+    for r in range(reps + 1):
+        restore()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        dev = 0.0
+        for e, wl in zip(engs, wls):
+            e.run(wl.first_step, wl.steps)
+            dev += e.last_run_stats()[0]
+        wall = time.perf_counter() - t
+        if r:                                            # the first pass is the warm-up
+            sep_wall.append(wall)
+            sep_dev.append(dev)
+    b = capi.Batch(0)
+    for e, wl in zip(engs, wls):
+        b.add(e, wl.first_step, wl.steps)
+    props = torch.cuda.get_device_properties(0)
+    key = f"{props.name}|sm{props.multi_processor_count}|batch256-rng4"
+    cache = json.loads(TUNED.read_text()) if TUNED.exists() else {}
+    tuned_now = key not in cache
+    if tuned_now:
+        shape, _ = b.tune()
+    else:
+        shape = cache[key]["shape"]
+        b.set_shape(**shape)
+    bat_wall, bat_dev = [], []
+    launches = 0
+    for r in range(reps + 1):
+        restore()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        b.run()
+        wall = time.perf_counter() - t
+        ms, nl, _ = b.stats()
+        if r:
+            bat_wall.append(wall)
+            bat_dev.append(ms)
+            launches += nl
+    b.close()
+    for e in engs:
+        e.close()
+    sep_v, bat_v = ps / statistics.median(sep_wall), ps / statistics.median(bat_wall)
+    return {
+        "workload": "batch of 256 ensembles: counts log-uniform in [1e3, 1e6], m in {1.5, 4.75} GeV, "
+                    "2piT Ds ~ U[2, 8], 500-2000 steps, half Bjorken (dtau 0.005), half 2+1D grids 201x201x100 "
+                    "(T0 ~ U[0.35, 0.55] GeV, sy/sx ~ U[0.7, 1]), Langevin+RTA, FP32",
+        "particles": sum(w.n for w in wls), "particle_steps": ps, "unit": "particle-steps/s",
+        "value": bat_v, "separate_value": sep_v, "speedup": bat_v / sep_v,
+        "value_device": ps / (statistics.median(bat_dev) * 1e-3),
+        "separate_value_device": ps / (statistics.median(sep_dev) * 1e-3),
+        "timing": "wall clock around one lim_batch_run (one CUDA-graph replay) vs around 256 lim_run calls; "
+                  "value_device: CUDA events of the graph vs the sum of the runs' event times; median of "
+                  f"{reps} after one warm-up, L2 flushed before each",
+        "shape": shape, "shape_source": "autotuned in this run (lim_batch_tune)" if tuned_now else
+                                         "autotuner result cached in langevinmedium.jl_b200/tuned_shapes.json",
+        "shape_key": key, "gpu_launches_per_run": launches // reps, "separate_launches_per_run": 2 * len(wls),
+    }
+
+
+def bench_adjoint(pkg, args):
+    """Forward + adjoint cost on the differentiation workload (2+1D grid, 1e6 charm,
+    2000 steps, checkpoints every 64 steps) against the plain forward."""
+    W, capi = pkg.workloads, pkg.capi
+    wl = W.adjoint_grid(N=1_000_000, steps=2000)
+    e = capi.Engine(0)
+    W.configure(e, wl)
+    e.initial_lab_boost()
+    e.state_save()
+    reps = max(1, min(args.steps, 3))
+    fwd, adj, fparts, rparts = [], [], [], []
+    for r in range(reps + 1):
+        e.state_restore()
+        e.run(1, wl.steps)
+        f_ms = e.last_run_stats()[0]
+        e.state_restore()
+        obs, G = e.adjoint(1, wl.steps, checkpoint_every=64)
+        a_f, a_r = e.adjoint_stats()
+        if r:
+            fwd.append(f_ms)
+            adj.append(a_f + a_r)
+            fparts.append(a_f)
+            rparts.append(a_r)
+    e.close()
+    f_ms, a_ms = statistics.median(fwd), statistics.median(adj)
+    return {
+        "workload": "2+1D grid medium, 1e6 charm, 2000 steps (dt 0.01), Langevin+RTA, FP32; d/d(a, b, s) of "
+                    "<pT>, <cos 2phi>, smoothed fraction pT > 5 GeV; 2piT Ds = a + b (T/0.155 - 1), a=3, b=2, s=1",
+        "checkpoint_every": 64, "plain_forward_ms": f_ms, "forward_plus_adjoint_ms": a_ms,
+        "checkpointed_forward_ms": statistics.median(fparts), "reverse_sweep_ms": statistics.median(rparts),
+        "cost_ratio": a_ms / f_ms, "obs": obs.tolist(), "grad": G.tolist(),
+        "timing": f"CUDA events, median of {reps} after one warm-up",
+    }
+
+
+def bench_grid(pkg, args, fma_rate):
+    """The 2+1D grid workload: 5e6 charm + 5e6 bottom, freeze-out at T < 0.155 GeV
+    (particles stop when they freeze out), 940 steps of 0.01 fm."""
+    W, capi = pkg.workloads, pkg.capi
+    wm = json.loads((Path(pkg.__file__).parent / "work_model.json").read_text())
+    i_alg = sum(sum(v.values()) for v in wm["workloads"]["grid2p1_langevin_rta_fo_fp32"]["items"].values())
+    fields = W.grid2p1_fields()
+    tot_ms, executed, nominal = 0.0, 0.0, 0
+    reps = max(1, min(args.steps, 3))
+    for m, rs in ((1.5, 3), (4.75, 13)):
+        wl = W.grid2p1(N=5_000_000, m=m, fields=fields, rng_seed=rs)
+        e = capi.Engine(0)
+        W.configure(e, wl)
+        e.initial_lab_boost()
+        e.state_save()
+        ms = []
+        for r in range(reps + 1):
+            e.state_restore()
+            e.run(wl.first_step, wl.steps)
+            if r:
+                ms.append(e.last_run_stats()[0])
+        f = e.download_freezeout()
+        frozen = f["flag"] != 0
+        st = np.where(frozen, np.ceil((f["tau"] - wl.params["t0"]) / wl.params["dt"] - 1e-9), wl.steps)
+        executed += float(np.minimum(st, wl.steps).sum())
+        nominal += wl.n * wl.steps
+        tot_ms += statistics.median(ms)
+        e.close()
+    rate = executed / (tot_ms * 1e-3)
+    return {
+        "workload": "2+1D grid 201x201x100 (T0 0.45 GeV, elliptic, radial u^r = tanh(0.05 r (tau - 0.6))), 5e6 charm "
+                    "+ 5e6 bottom, Langevin+RTA, freeze-out latch at T < 0.155 GeV, particles stop at freeze-out, "
+                    "940 steps, FP32",
+        "unit": "particle-steps/s", "value_executed": rate, "value_nominal": nominal / (tot_ms * 1e-3),
+        "executed_particle_steps": executed, "nominal_particle_steps": nominal, "kernel_ms": tot_ms,
+        "roofline": {"bound": "issue", "unit": "Ginst/s", "algorithmic_inst_per_particle_step": i_alg,
+                     "achieved": i_alg * rate / 1e9, "peak": fma_rate / 1e9, "frac": i_alg * rate / fma_rate,
+                     "peak_source": "FP32 FMA issue probe (lim_probe_fma_rate), this run"},
+        "timing": f"CUDA events of the runs (table, step and compaction kernels), median of {reps} after one warm-up",
+    }
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
     import torch.distributed as dist
@@ -316,6 +487,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                "sample": f"{ncpu} charm quarks x 1880 steps of the same workload, FP64 restatement (oracle/), "
                          f"{info['seconds']:.1f} s"}
+    extra = {}
+    if world == 1 and not args.quick:
+        extra["batched"] = bench_batched(pkg, args, flush)
+        extra["adjoint"] = bench_adjoint(pkg, args)
+        extra["grid2p1"] = bench_grid(pkg, args, fma_rate)
+    elif world > 1:
+        extra["batched"] = extra["adjoint"] = extra["grid2p1"] = {"skipped": "measured in the one-GPU run"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -336,6 +514,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                                                                        max(float(sums[0]), 1.0)))},
         }
         line["observables"]["count"] = float(sums[0])
+        line.update(extra)
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
@@ -351,6 +530,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--particles", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="only the headline workload (no batched/adjoint/grid legs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -18,8 +18,9 @@
 //   G streaming                   x' = x + dt p5 / E5
 // with u the spatial fluid four-velocity, gamma = sqrt(1 + u.u), c = 1/(1 + gamma),
 // which is the step of lim_step.cuh (its frame change is this map, up to the
-// reference's 1e-10 under the square root of gamma) and is smooth in u at u = 0.  Intermediates are re-evaluated in FP32 from the taped state; slopes of
-// the tabulated functions come from tables differenced in FP64 on the host.
+// reference's 1e-10 under the square root of gamma) and is smooth in u at u = 0.
+// Intermediates are re-evaluated in FP32 from the taped state; slopes of the
+// tabulated functions come from tables differenced in FP64 on the host.
 #include "lim_internal.h"
 #include "lim_particle.cuh"
 
