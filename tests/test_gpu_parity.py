@@ -124,14 +124,16 @@ def check_fo_outputs(lmb, orc, wl, name, record):
     both = (gf == 1) & (of == 1)
     assert_parity(tag + " live", g, o, TOL["fp32"], floor=1.0, mask=live)
     # The latch interpolates to T = Tfo with frac = (T_prev - Tfo)/(T_prev - T), whose
-    # condition number is T/(T_prev - T) ~ 1e2-1e3: FP32-level trajectory differences
-    # reach the latched outputs amplified by it.  Gate: 99th percentile 1e-5, max 1e-4.
+    # condition number T/(T_prev - T) is ~1e2-1e3 for most particles and unbounded for a
+    # particle that moves along the Tfo isotherm: FP32-level trajectory differences reach
+    # the latched outputs amplified by it, bounded by the one-step change of the state
+    # (~1e-2).  Gate: 99th percentile 1e-5, max 1e-3.
     ep = parity(g["fo"]["mom"][:, both], o["fo_mom"][:, both], 0.3, 1.0)
     ex = parity(g["fo"]["pos"][:, both], o["fo_pos"][:, both], 1.0, 1.0)
     et = parity(g["fo"]["tau"][both], o["fo_tau"][both], 1.0, 1.0)
     print(f"{tag} latched: x max {ex[0]:.3g} p99 {ex[1]:.3g} | p max {ep[0]:.3g} p99 {ep[1]:.3g} | tau max {et[0]:.3g}")
     for e in (ep, ex, et):
-        assert e[1] <= TOL["fp32"] and e[0] <= 10 * TOL["fp32"], (tag, ep, ex, et)
+        assert e[1] <= TOL["fp32"] and e[0] <= 100 * TOL["fp32"], (tag, ep, ex, et)
 
 
 def test_fp64_recorded_noise_matches_regenerated(lmb, orc):
