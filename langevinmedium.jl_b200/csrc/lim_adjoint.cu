@@ -93,12 +93,12 @@ __device__ __forceinline__ float invcdf_lookup_dT(const KParams<float>& kp, uint
 
 // Vector-Jacobian product of the boost p' = p + c (p.u) u + sg E u (u in the x-y plane):
 // b (the cotangent of p') -> the cotangent of p, and the cotangent of u added to ub.
-__device__ __forceinline__ void boost_vjp(float sg, const float (&p)[3], float E, float ux, float uy, float gam, float c,
-                                          const float (&b)[3], float (&bp)[3], float (&ub)[2])
+__device__ __forceinline__ void boost_vjp(float sg, const float (&p)[3], float E, float iE, float ux, float uy,
+                                          float gam, float c, const float (&b)[3], float (&bp)[3], float (&ub)[2])
 {
     const float A = b[0] * ux + b[1] * uy;
     const float pu = p[0] * ux + p[1] * uy;
-    const float sAE = sg * A / E;
+    const float sAE = sg * A * iE;
     bp[0] = b[0] + c * A * ux + sAE * p[0];
     bp[1] = b[1] + c * A * uy + sAE * p[1];
     bp[2] = b[2] + sAE * p[2];
@@ -148,10 +148,19 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
     // ---- D. kick
     const float Tk = jmax0(T);
     const SplIdx<float> sd = spline_index(Tk, kp.drag_Tmin, kp.drag_invdT, kp.n_drag);
-    const float tau = kp.DsT <= 0.0f ? 0.0f : spline_at(kp.drag, sd);
+    float tau = 0.0f, slope = 0.0f, dta = 0.0f, dtb = 0.0f;
+    if (sd.mode != 2 && kp.DsT > 0.0f) {       // one cell record: value, slope, d/da, d/db
+        const bool lin = sd.mode == 0;
+        const float4* c = kp.adj_drag + (lin ? 2 * sd.i : 0);
+        const float4 q0 = __ldg(c), q1 = __ldg(c + 1);
+        const float t = lin ? sd.t : 0.0f;
+        tau = q0.x + t * q0.y;
+        dta = q0.z + t * q0.w;
+        dtb = q1.x + t * q1.y;
+        slope = lin ? q1.z : 0.0f;
+    }
     const bool ok = tau > 0.0f && isfinite(tau);
     float E1 = 0.0f, xk = 0.0f, a = 1.0f, q = 0.0f, amp = 0.0f;
-    float slope = 0.0f, dta = 0.0f, dtb = 0.0f;
     float p3[3] = { p2[0], p2[1], p2[2] };
     if (ok) {
         E1 = sqrtf(p2[0] * p2[0] + p2[1] * p2[1] + p2[2] * p2[2] + m * m);
@@ -162,9 +171,6 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
         amp = (dt > 0.0f && xk > 0.0f) ? sqrtf(Tk * E1 * q) : 0.0f;
 #pragma unroll
         for (int d = 0; d < 3; ++d) p3[d] = p2[d] + em1 * p2[d] + amp * xi[d];
-        if (sd.mode == 0) slope = __ldg(kp.drag_slope + sd.i);
-        dta = spline_at(kp.drag_da, sd);
-        dtb = spline_at(kp.drag_db, sd);
     }
     // ---- E. RTA with the recorded indicator
     bool col = false;
@@ -192,11 +198,14 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
     const float iE5 = 1.0f / E5;
 
     // partials shared by the cotangents
-    const float da_dE1 = ok ? a * xk / E1 : 0.0f;
-    const float damp_dE1 = (ok && q > 0.0f) ? amp / (2.0f * E1) - amp * a * a * xk / (q * E1) : 0.0f;
-    const float da_dtau = ok ? a * xk / tau : 0.0f;
-    const float damp_dtau = (ok && q > 0.0f) ? -amp * a * a * xk / (q * tau) : 0.0f;
-    const float damp_dT = (ok && Tk > 0.0f) ? amp / (2.0f * Tk) : 0.0f;
+    const float iE0 = flow ? 1.0f / E0 : 0.0f, iE4 = flow ? 1.0f / E4 : 0.0f;
+    const float iE1 = ok ? 1.0f / E1 : 0.0f, itau = ok ? 1.0f / tau : 0.0f;
+    const float aaxq = (ok && q > 0.0f) ? amp * a * a * xk / q : 0.0f;     // amp a^2 x / q
+    const float da_dE1 = a * xk * iE1;
+    const float damp_dE1 = (0.5f * amp - aaxq) * iE1;
+    const float da_dtau = a * xk * itau;
+    const float damp_dtau = -aaxq * itau;
+    const float damp_dT = (ok && Tk > 0.0f) ? 0.5f * amp / Tk : 0.0f;
 #pragma unroll
     for (int o = 0; o < NC; ++o) {
         // G^T
@@ -208,7 +217,7 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
         // F^T
         float ub[2] = { 0.0f, 0.0f };
         float b4[3];
-        if (flow) boost_vjp(1.0f, p4, E4, ux, uy, gam, c, b, b4, ub);
+        if (flow) boost_vjp(1.0f, p4, E4, iE4, ux, uy, gam, c, b, b4, ub);
         else { b4[0] = b[0]; b4[1] = b[1]; b4[2] = b[2]; }
         // E^T
         float Tb = 0.0f, b3[3];
@@ -223,7 +232,7 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
         if (ok) {
             const float Sa = b3[0] * p2[0] + b3[1] * p2[1] + b3[2] * p2[2];
             const float Sx = b3[0] * xi[0] + b3[1] * xi[1] + b3[2] * xi[2];
-            const float cE = (Sa * da_dE1 + Sx * damp_dE1) / E1;
+            const float cE = (Sa * da_dE1 + Sx * damp_dE1) * iE1;
 #pragma unroll
             for (int d = 0; d < 3; ++d) b2[d] = a * b3[d] + cE * p2[d];
             const float taub = Sa * da_dtau + Sx * damp_dtau;
@@ -235,7 +244,7 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
         float b1[3] = { b2[0], b2[1], kp.redshift ? b2[2] * zf : b2[2] };
         // B^T
         float b0[3];
-        if (flow) boost_vjp(-1.0f, ps, E0, ux, uy, gam, c, b1, b0, ub);
+        if (flow) boost_vjp(-1.0f, ps, E0, iE0, ux, uy, gam, c, b1, b0, ub);
         else { b0[0] = b1[0]; b0[1] = b1[1]; b0[2] = b1[2]; }
         // T = s Tf, Tk = max(T, 0)
         if (!(T > 0.0f)) Tb = 0.0f;
@@ -295,8 +304,10 @@ k_adjoint_seed(const KParams<float> kp, const AdjointArgs aa)
 }
 
 // Steps [s0, s1) backwards from the tape (index s - s0).
+// At most 102 registers (five 128-thread blocks per SM): 6 % faster than the natural
+// 124 on the 2+1D workload.
 template <int MED>
-__global__ void __launch_bounds__(kAdjBlock)
+__global__ void __launch_bounds__(kAdjBlock, 5)
 k_adjoint_rev(const KParams<float> kp, const AdjointArgs aa, int64_t s0, int64_t s1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -313,11 +324,12 @@ k_adjoint_rev(const KParams<float> kp, const AdjointArgs aa, int64_t s0, int64_t
     }
     const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<float>* __restrict__ tab = (const StepRec<float>*)kp.steps - kp.step_base;
-    for (int64_t s = s1 - 1; s >= s0; --s) {
-        const float* t = kp.tape + (size_t)(s - s0) * kTapeFields * n + i;
-        const float xs[2] = { t[0], t[n] };
-        const float ps[3] = { t[2 * n], t[3 * n], t[4 * n] };
-        const float xi[3] = { t[5 * n], t[6 * n], t[7 * n] };
+    const float4* t = reinterpret_cast<const float4*>(kp.tape) + (size_t)(s1 - 1 - s0) * 2 * n + i;
+    for (int64_t s = s1 - 1; s >= s0; --s, t -= 2 * n) {
+        const float4 ta = __ldg(t), tb = __ldg(t + n);
+        const float xs[2] = { ta.x, ta.y };
+        const float ps[3] = { ta.z, ta.w, tb.x };
+        const float xi[3] = { tb.y, tb.z, tb.w };
         const StepRec<float> sr = tab[s];
         adjoint_step<MED, kAdjCot>(kp, sr, s, i, nk, xs, ps, xi, lx, lp, g);
     }

@@ -71,11 +71,20 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
     // slopes of the tabulated functions, differenced in FP64 (FP32 node differences
     // lose ~eps / (relative step) to cancellation)
     {
+        // per drag cell: (tau_i, tau_i+1 - tau_i, a_i, a_i+1 - a_i), (b_i, b_i+1 - b_i, slope_i, 0)
         const std::vector<double>& v = c->spl[0];
-        std::vector<float> sl(std::max<size_t>(v.size(), 2) - 1, 0.0f);
-        for (size_t k = 0; k + 1 < v.size(); ++k) sl[k] = (float)((v[k + 1] - v[k]) * c->spl_invdT[0]);
-        if ((rc = ctx_alloc(c, c->d_adj_slope, sl.size() * sizeof(float)))) return rc;
-        LIM_ACUDA(c, cudaMemcpy(c->d_adj_slope.p, sl.data(), sl.size() * sizeof(float), cudaMemcpyHostToDevice));
+        const std::vector<double>& A = c->spl[2];
+        const std::vector<double>& B = c->spl[3];
+        const size_t cells = std::max<size_t>(v.size(), 2) - 1;
+        std::vector<float4> tab(2 * cells);
+        for (size_t k = 0; k < cells; ++k) {
+            const size_t k1 = std::min(k + 1, v.size() - 1);
+            const double dv = v[k1] - v[k], da = A[k1] - A[k], dbv = B[k1] - B[k];
+            tab[2 * k] = make_float4((float)v[k], (float)dv, (float)A[k], (float)da);
+            tab[2 * k + 1] = make_float4((float)B[k], (float)dbv, (float)(dv * c->spl_invdT[0]), 0.0f);
+        }
+        if ((rc = ctx_alloc(c, c->d_adj_slope, tab.size() * sizeof(float4)))) return rc;
+        LIM_ACUDA(c, cudaMemcpy(c->d_adj_slope.p, tab.data(), tab.size() * sizeof(float4), cudaMemcpyHostToDevice));
         const int64_t nU = c->nU, nT = c->nT;
         std::vector<float> dT((size_t)std::max<int64_t>(nT - 1, 1) * (size_t)std::max<int64_t>(nU, 1), 0.0f);
         if (!c->icdf.empty())
@@ -89,7 +98,7 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
     kp.steps = c->d_adj_table.p;
     kp.step_base = first_step;
     kp.step_cap = nsteps;
-    kp.drag_slope = (const float*)c->d_adj_slope.p;
+    kp.adj_drag = (const float4*)c->d_adj_slope.p;
     kp.icdf_dT = (const float*)c->d_adj_icdt.p;
     LIM_ACUDA(c, launch_step_table<float>(kp, 0, first_step, first_step + nsteps, c->stream));
     const int block = c->P.block_size > 0 ? (int)c->P.block_size : 256;

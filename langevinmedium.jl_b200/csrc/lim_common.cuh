@@ -10,7 +10,7 @@ namespace lim {
 constexpr double kEps = 2.220446049250313e-16;   // Julia eps()
 constexpr double kFmGeV = 1.0 / 0.197327;        // constants.jl:13,23
 constexpr int kNoiseSlots = 11;
-constexpr int kTapeFields = 8;   // adjoint tape per step: x (2), p (3), momentum normals (3), FP32
+constexpr int kTapeFields = 8;   // adjoint tape per step: two float4, (x0, x1, p0, p1) and (p2, xi0, xi1, xi2)
 enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4 };
 enum { MED_RT = 0, MED_BJORKEN = 1, MED_GRID = 2 };
 enum { COLL_LANGEVIN = 0, COLL_RTA = 1, COLL_LANGEVIN_RTA = 2, COLL_FLUID = 3 };
@@ -83,11 +83,12 @@ struct alignas(16) KParams {
     // (bit (s - rta_first) % 32 of word [(s - rta_first) / 32][particle], zeroed before),
     // 2 replays them instead of comparing u_collide with the collision probability
     uint32_t* rta_bits; int rta_mode; int64_t rta_first, rta_steps;
-    // derivative tables of the drag spline w.r.t. two parameters of D_s(T) (same T grid),
-    // the drag spline's cell slopes and the inverse CDF's T differences (both formed in
-    // FP64 on the host), and the adjoint's tape of steps [tape_first, ...)
+    // derivative tables of the drag spline w.r.t. two parameters of D_s(T) (same T grid);
+    // for the adjoint: per drag cell two float4 (tau_i, dtau_i, a_i, da_i), (b_i, db_i,
+    // dtau_i invdT, 0) with the differences to cell i+1 formed in FP64, the inverse
+    // CDF's T differences, and the tape of steps [tape_first, ...)
     const R* drag_da; const R* drag_db;
-    const R* drag_slope; const R* icdf_dT;
+    const float4* adj_drag; const R* icdf_dT;
     float* tape; int64_t tape_first;
 };
 

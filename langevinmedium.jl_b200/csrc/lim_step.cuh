@@ -261,7 +261,8 @@ __device__ __forceinline__ void rec_slot(const KParams<R>& kp, int64_t s, int64_
     if (REC == 1 && s >= kp.rec_first && s < kp.rec_first + kp.rec_steps)
         kp.rec[((s - kp.rec_first) * kNoiseSlots + slot) * kp.n + i] = (double)val;
     if (REC == 2 && slot < 3)
-        kp.tape[((s - kp.tape_first) * kTapeFields + 5 + slot) * kp.n + i] = (float)val;
+        reinterpret_cast<float*>(reinterpret_cast<float4*>(kp.tape) + ((s - kp.tape_first) * 2 + 1) * kp.n + i)[1 + slot] =
+            (float)val;
 }
 
 // expm1(-x) for x >= 0: Taylor series below 0.05 (truncation < 1e-11 relative),
