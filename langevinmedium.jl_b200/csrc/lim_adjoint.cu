@@ -276,6 +276,17 @@ __device__ __forceinline__ void final_observables(double px, double py, double c
 
 }  // namespace
 
+// The forward pass: steps [s0, s1) in one launch, the state checkpointed in registers
+// every ckpt_every steps (no segment launches, no copies).
+template <int MED>
+__global__ void __launch_bounds__(256, 3)
+k_ckpt_forward(const KParams<float> kp, int64_t s0, int64_t s1)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kp.n) return;
+    cart_particle<3, false, float, MED, 2, 3>(kp, kp.rk, i, s0, s1);
+}
+
 // Recomputes steps [s0, s1) from the checkpoint the parameters point at, taping them.
 template <int MED>
 __global__ void __launch_bounds__(256)
@@ -325,13 +336,17 @@ k_adjoint_rev(const KParams<float> kp, const AdjointArgs aa, int64_t s0, int64_t
     const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<float>* __restrict__ tab = (const StepRec<float>*)kp.steps - kp.step_base;
     const float4* t = reinterpret_cast<const float4*>(kp.tape) + (size_t)(s1 - 1 - s0) * 2 * n + i;
+    float4 ta = __ldg(t), tb = __ldg(t + n);
     for (int64_t s = s1 - 1; s >= s0; --s, t -= 2 * n) {
-        const float4 ta = __ldg(t), tb = __ldg(t + n);
+        float4 na = ta, nb = tb;              // the next (earlier) step's record, loaded ahead
+        if (s > s0) { na = __ldg(t - 2 * n); nb = __ldg(t - n); }
         const float xs[2] = { ta.x, ta.y };
         const float ps[3] = { ta.z, ta.w, tb.x };
         const float xi[3] = { tb.y, tb.z, tb.w };
         const StepRec<float> sr = tab[s];
         adjoint_step<MED, kAdjCot>(kp, sr, s, i, nk, xs, ps, xi, lx, lp, g);
+        ta = na;
+        tb = nb;
     }
 #pragma unroll
     for (int o = 0; o < kAdjCot; ++o) {
@@ -380,14 +395,17 @@ k_adjoint_gsum(const KParams<float> kp, const AdjointArgs aa)
     }
 }
 
-// Fixed-order total of the block partials.
+// Fixed-order total of the block partials: one warp per output, lane-strided sums
+// combined by a fixed shuffle tree.
 __global__ void k_adjoint_total(const double* __restrict__ partials, int64_t nblocks, double* out)
 {
-    const int k = threadIdx.x;
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k >= kAdjOut) return;
     double t = 0.0;
-    for (int64_t b = 0; b < nblocks; ++b) t += partials[b * kAdjOut + k];
-    out[k] = t;
+    for (int64_t b = lane; b < nblocks; b += 32) t += partials[b * kAdjOut + k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+    if (lane == 0) out[k] = t;
 }
 
 static unsigned blocks_of(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -396,6 +414,15 @@ cudaError_t launch_adjoint_seed(const KParams<float>& kp, const AdjointArgs& aa,
 {
     if (kp.n == 0) return cudaSuccess;
     k_adjoint_seed<<<blocks_of(kp.n, kAdjBlock), kAdjBlock, 0, st>>>(kp, aa);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_forward(const KParams<float>& kp, int64_t s0, int64_t s1, cudaStream_t st)
+{
+    if (kp.n == 0) return cudaSuccess;
+    if (kp.med.kind == MED_GRID) k_ckpt_forward<MED_GRID><<<blocks_of(kp.n, 256), 256, 0, st>>>(kp, s0, s1);
+    else if (kp.med.kind == MED_BJORKEN) k_ckpt_forward<MED_BJORKEN><<<blocks_of(kp.n, 256), 256, 0, st>>>(kp, s0, s1);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
@@ -426,7 +453,7 @@ cudaError_t launch_adjoint_total(const KParams<float>& kp, const AdjointArgs& aa
     k_adjoint_gsum<<<(unsigned)nb, kAdjBlock, 0, st>>>(kp, aa);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_adjoint_total<<<1, 32, 0, st>>>(aa.partials, nb, out);
+    k_adjoint_total<<<1, 32 * kAdjOut, 0, st>>>(aa.partials, nb, out);
     return cudaGetLastError();
 }
 
