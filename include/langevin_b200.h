@@ -144,8 +144,8 @@ int lim_set_medium_bjorken(lim_ctx* ctx, double T0, double tau0, double power, d
 
 /* 2+1D medium on a uniform grid: fields in FP32, row-major [it][iy][ix]
  * (ix fastest), node (ix, iy, it) at (x0 + ix*dx, y0 + iy*dy, tau0 + it*dtau).
- * u^x, u^y are the spatial components of the fluid four-velocity: the flow speed is
- * |u| / sqrt(1 + |u|^2) along u / |u|. */
+ * u^x, u^y are the flow velocity components (as the reference's VelocityEvolution is a
+ * velocity, kernels_cpu.jl:80,105): speed |u| along u / |u|. */
 int lim_set_medium_grid(lim_ctx* ctx,
                         int64_t nx, int64_t ny, int64_t nt,
                         double x0, double dx, double y0, double dy,

@@ -16,9 +16,11 @@
 //   C Bjorken redshift of p_z     D OU kick     p3 = a(p2) p2 + amp(p2, T, tau) xi
 //   E RTA resample (fixed)        F lab boost   p5 = p4 + c (p4.u) u + E u
 //   G streaming                   x' = x + dt p5 / E5
-// with u the spatial fluid four-velocity, gamma = sqrt(1 + u.u), c = 1/(1 + gamma),
-// which is the step of lim_step.cuh (its frame change is this map, up to the
-// reference's 1e-10 under the square root of gamma) and is smooth in u at u = 0.
+// with u = g V the spatial fluid four-velocity formed from the grid's flow velocity V
+// (g = 1/sqrt(1 - V.V)), gamma = sqrt(1 + u.u) = g, c = 1/(1 + gamma): the step of
+// lim_step.cuh (its frame change is this map, up to the reference's 1e-10 under the
+// square root of gamma), smooth in V at V = 0; the cotangent of u maps back to the
+// velocity field through du/dV = g I + g^3 V V^T.
 // Intermediates are re-evaluated in FP32 from the taped state; slopes of the
 // tabulated functions come from tables differenced in FP64 on the host.
 #include "lim_internal.h"
@@ -28,7 +30,7 @@ namespace lim {
 
 namespace {
 
-// Trilinear (T, u^x, u^y) at (x, y) and their gradients in x and y (zero along an
+// Trilinear (T, v^x, v^y) at (x, y) and their gradients in x and y (zero along an
 // axis where the query is clamped to the grid).
 __device__ __forceinline__ void grid_lookup_grad(const MediumDev<float>& md, const StepRec<float>& sr, float xq, float yq,
                                                  float& T, float& ux, float& uy, float (&dT)[2], float (&dux)[2],
@@ -131,12 +133,15 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
     // ---- A. medium
     float Tf, ux = 0.0f, uy = 0.0f;
     float dT[2] = { 0.0f, 0.0f }, dux[2] = { 0.0f, 0.0f }, duy[2] = { 0.0f, 0.0f };
-    if (MED == MED_GRID) grid_lookup_grad(kp.med, sr, xs[0], xs[1], Tf, ux, uy, dT, dux, duy);
+    float vx = 0.0f, vy = 0.0f;                 // the grid's flow velocity
+    if (MED == MED_GRID) grid_lookup_grad(kp.med, sr, xs[0], xs[1], Tf, vx, vy, dT, dux, duy);
     else Tf = sr.T_bj;
     const float sc = kp.med.T_scale;
     const float T = Tf * sc;
-    const bool flow = MED == MED_GRID && !(sqrtf(ux * ux + uy * uy) < (float)kEps);
-    const float gam = sqrtf(1.0f + ux * ux + uy * uy), c = 1.0f / (1.0f + gam);
+    const bool flow = MED == MED_GRID && !(sqrtf(vx * vx + vy * vy) < (float)kEps);
+    const float gam = rsqrtf(1.0f - (vx * vx + vy * vy)), c = 1.0f / (1.0f + gam);
+    ux = gam * vx;                              // four-velocity
+    uy = gam * vy;
     // ---- B. rest boost
     float p1[3], E0 = 0.0f;
     if (flow) boost_fwd(-1.0f, ps, m, ux, uy, c, p1, E0);
@@ -250,9 +255,12 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
         if (!(T > 0.0f)) Tb = 0.0f;
         g[o][2] += Tb * Tf;
         const float Tfb = Tb * sc;
+        // u = g V: the cotangent of the velocity is g ub + g^3 V (ub . V)
+        const float uV = gam * gam * gam * (ub[0] * vx + ub[1] * vy);
+        const float vb0 = gam * ub[0] + uV * vx, vb1 = gam * ub[1] + uV * vy;
         // A^T
-        lx[o][0] += Tfb * dT[0] + ub[0] * dux[0] + ub[1] * duy[0];
-        lx[o][1] += Tfb * dT[1] + ub[0] * dux[1] + ub[1] * duy[1];
+        lx[o][0] += Tfb * dT[0] + vb0 * dux[0] + vb1 * duy[0];
+        lx[o][1] += Tfb * dT[1] + vb0 * dux[1] + vb1 * duy[1];
         lp[o][0] = b0[0]; lp[o][1] = b0[1]; lp[o][2] = b0[2];
     }
 }
@@ -275,17 +283,6 @@ __device__ __forceinline__ void final_observables(double px, double py, double c
 }
 
 }  // namespace
-
-// The forward pass: steps [s0, s1) in one launch, the state checkpointed in registers
-// every ckpt_every steps (no segment launches, no copies).
-template <int MED>
-__global__ void __launch_bounds__(256, 3)
-k_ckpt_forward(const KParams<float> kp, int64_t s0, int64_t s1)
-{
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kp.n) return;
-    cart_particle<3, false, float, MED, 2, 3>(kp, kp.rk, i, s0, s1);
-}
 
 // Recomputes steps [s0, s1) from the checkpoint the parameters point at, taping them.
 template <int MED>
@@ -336,17 +333,13 @@ k_adjoint_rev(const KParams<float> kp, const AdjointArgs aa, int64_t s0, int64_t
     const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<float>* __restrict__ tab = (const StepRec<float>*)kp.steps - kp.step_base;
     const float4* t = reinterpret_cast<const float4*>(kp.tape) + (size_t)(s1 - 1 - s0) * 2 * n + i;
-    float4 ta = __ldg(t), tb = __ldg(t + n);
     for (int64_t s = s1 - 1; s >= s0; --s, t -= 2 * n) {
-        float4 na = ta, nb = tb;              // the next (earlier) step's record, loaded ahead
-        if (s > s0) { na = __ldg(t - 2 * n); nb = __ldg(t - n); }
+        const float4 ta = __ldg(t), tb = __ldg(t + n);
         const float xs[2] = { ta.x, ta.y };
         const float ps[3] = { ta.z, ta.w, tb.x };
         const float xi[3] = { tb.y, tb.z, tb.w };
         const StepRec<float> sr = tab[s];
         adjoint_step<MED, kAdjCot>(kp, sr, s, i, nk, xs, ps, xi, lx, lp, g);
-        ta = na;
-        tb = nb;
     }
 #pragma unroll
     for (int o = 0; o < kAdjCot; ++o) {
@@ -414,15 +407,6 @@ cudaError_t launch_adjoint_seed(const KParams<float>& kp, const AdjointArgs& aa,
 {
     if (kp.n == 0) return cudaSuccess;
     k_adjoint_seed<<<blocks_of(kp.n, kAdjBlock), kAdjBlock, 0, st>>>(kp, aa);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_adjoint_forward(const KParams<float>& kp, int64_t s0, int64_t s1, cudaStream_t st)
-{
-    if (kp.n == 0) return cudaSuccess;
-    if (kp.med.kind == MED_GRID) k_ckpt_forward<MED_GRID><<<blocks_of(kp.n, 256), 256, 0, st>>>(kp, s0, s1);
-    else if (kp.med.kind == MED_BJORKEN) k_ckpt_forward<MED_BJORKEN><<<blocks_of(kp.n, 256), 256, 0, st>>>(kp, s0, s1);
-    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 

@@ -105,15 +105,21 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
     cudaEvent_t e0 = c->ev0, e1 = c->ev1, e2 = nullptr;
     LIM_ACUDA(c, cudaEventCreate(&e2));
     LIM_ACUDA(c, cudaEventRecord(e0, c->stream));
-    // forward: one launch over all steps, the state checkpointed every K steps
+    // forward: checkpoint, then the segment's steps (one launch per segment: measured
+    // faster than one launch that checkpoints from inside, whose extra live values cost
+    // occupancy)
     const size_t fb = (size_t)n * sizeof(float), db = (size_t)n * sizeof(double);
-    (void)block;
-    kp.ckpt = (char*)c->d_adj_ckpt.p;
-    kp.ckpt_every = K;
-    kp.ckpt_seg_bytes = (int64_t)seg_bytes;
-    kp.tape_first = first_step;
-    LIM_ACUDA(c, launch_adjoint_forward(kp, first_step, first_step + nsteps, c->stream));
-    kp.ckpt = nullptr;
+    for (int64_t seg = 0; seg < nseg; ++seg) {
+        char* cb = (char*)c->d_adj_ckpt.p + (size_t)seg * seg_bytes;
+        for (int d = 0; d < 2; ++d) {
+            LIM_ACUDA(c, cudaMemcpyAsync(cb + d * fb, kp.x[d], fb, cudaMemcpyDeviceToDevice, c->stream));
+            LIM_ACUDA(c, cudaMemcpyAsync(cb + (2 + d) * fb, kp.xlo[d], fb, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        for (int d = 0; d < 3; ++d)
+            LIM_ACUDA(c, cudaMemcpyAsync(cb + 4 * fb + d * db, kp.p[d], db, cudaMemcpyDeviceToDevice, c->stream));
+        const int64_t s0 = first_step + seg * K, s1 = std::min(s0 + K, first_step + nsteps);
+        LIM_ACUDA(c, launch_steps_in_table<float>(kp, s0, s1, block, c->stream));
+    }
     LIM_ACUDA(c, cudaEventRecord(e1, c->stream));
     // reverse sweep: seeds at the final state, then segment by segment from the last
     AdjointArgs aa;

@@ -90,9 +90,6 @@ struct alignas(16) KParams {
     const R* drag_da; const R* drag_db;
     const float4* adj_drag; const R* icdf_dT;
     float* tape; int64_t tape_first;
-    // checkpoints written by the adjoint's forward pass: the state before step
-    // tape_first + k ckpt_every at ckpt + k ckpt_seg_bytes (x[2], x_lo[2] float, p[3] double)
-    char* ckpt; int64_t ckpt_every; int64_t ckpt_seg_bytes;
 };
 
 // ---------------------------------------------------------------------------

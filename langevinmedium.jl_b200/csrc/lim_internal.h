@@ -77,7 +77,6 @@ struct AdjointArgs {
     double* partials;            // [nblocks][kAdjOut]
 };
 cudaError_t launch_adjoint_seed(const KParams<float>& kp, const AdjointArgs& aa, cudaStream_t st);
-cudaError_t launch_adjoint_forward(const KParams<float>& kp, int64_t s0, int64_t s1, cudaStream_t st);
 cudaError_t launch_adjoint_tape(const KParams<float>& kp, int64_t s0, int64_t s1, cudaStream_t st);
 cudaError_t launch_adjoint_rev(const KParams<float>& kp, const AdjointArgs& aa, int64_t s0, int64_t s1, cudaStream_t st);
 cudaError_t launch_adjoint_total(const KParams<float>& kp, const AdjointArgs& aa, double* out, cudaStream_t st);

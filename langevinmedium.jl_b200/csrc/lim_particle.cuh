@@ -65,22 +65,8 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     }
     const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
-    int64_t ck_left = 0, ck_seg = 0;          // REC == 3: steps to the next checkpoint
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && flag != 0.0) break;
-        if (REC == 3) {                   // the adjoint's forward pass: checkpoint every ckpt_every steps
-            if (ck_left == 0) {
-                const int64_t n = kp.n;
-                char* cb = kp.ckpt + ck_seg * kp.ckpt_seg_bytes;
-                float* f = reinterpret_cast<float*>(cb);
-                double* dp = reinterpret_cast<double*>(cb + 16 * n);
-                f[i] = (float)x[0]; f[n + i] = (float)x[1]; f[2 * n + i] = xl[0]; f[3 * n + i] = xl[1];
-                dp[i] = p[0]; dp[n + i] = p[1]; dp[2 * n + i] = p[2];
-                ck_left = kp.ckpt_every;
-                ++ck_seg;
-            }
-            --ck_left;
-        }
         const StepRec<R> sr = tab[s];
         if (REC == 2) {                   // the adjoint's tape: the pre-step state (the normals follow)
             float4* t = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 2 * kp.n + i;

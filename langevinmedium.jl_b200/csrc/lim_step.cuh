@@ -178,12 +178,12 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     Local<R> L;
     L.nx = R(0); L.ny = R(0); L.v = R(0);
     if (MED == MED_GRID) {
-        // the grid holds the spatial four-velocity (u^x, u^y): speed |u| / sqrt(1 + u^2)
+        // the grid holds the flow velocity (v^x, v^y), as the reference's (r, t) tables do
         R ux, uy;
         grid_lookup(kp.med, sr, x[0], x[1], L.T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
         L.boost = !(u < R(kEps));
-        L.v = u / sqrt(fma(u, u, R(1)));
+        L.v = u;
         if (L.boost) { L.nx = ux / u; L.ny = uy / u; }
     } else if (MED == MED_BJORKEN && fp32) {
         // zero flow: in FP32 the boost is the identity (gamma(0) rounds to 1)
@@ -441,8 +441,7 @@ __device__ __forceinline__ void set_to_fluid(const KParams<R>& kp, const StepRec
         grid_lookup(kp.med, sr, x[0], x[1], T, ux, uy);
         R u = sqrt(ux * ux + uy * uy);
         if (u < R(kEps)) { p[0] = 0.0; p[1] = 0.0; return; }
-        const R v = u / sqrt(fma(u, u, R(1)));          // four-velocity -> speed
-        R vc = kp.rel ? jclamp(v, -vmax, vmax) : v;
+        R vc = kp.rel ? jclamp(u, -vmax, vmax) : u;
         R g = kp.rel ? R(1) / sqrt(R(1) - vc * vc + R(1e-10)) : R(1);
         p[0] = (double)(m * g * vc * (ux / u));
         p[1] = (double)(m * g * vc * (uy / u));

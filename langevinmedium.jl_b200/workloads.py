@@ -12,9 +12,9 @@ medium from the same description.
                 Langevin + RTA with τ_R = 5 (η/s)/T, η/s = 0.16, Δτ = 0.005 (1880 steps),
                 p_T ∝ (p_T²+4)^-3 per d²p_T, φ uniform, rapidity uniform in [-1,1].
   grid2p1     — 201×201 cells at 0.1 fm, 100 τ slices 0.6 → 10 fm/c, elliptic Gaussian
-                T0 = 0.45 GeV (σx 3.0, σy 2.4 fm) × (0.6/τ)^(1/3), radial four-velocity
-                u^r = tanh(0.05 r (τ-0.6)) (fields hold u^x, u^y; speed u/sqrt(1+u²)),
-                freeze-out latch at T < 0.155 GeV, Δt = 0.01.
+                T0 = 0.45 GeV (σx 3.0, σy 2.4 fm) × (0.6/τ)^(1/3), radial flow
+                u^r = tanh(0.05 r (τ-0.6)) read as the flow velocity (the reference's
+                velocity fields are velocities), freeze-out latch at T < 0.155 GeV, Δt = 0.01.
   adjoint_grid — the grid medium for pathwise gradients: 1e6 charm, 2000 steps, no
                 freeze-out, 2πT·D_s = a + b (T/0.155 - 1) and a temperature scale s.
   batch       — 256 independent ensembles (counts log-uniform in [1e3, 1e6], charm or

@@ -416,11 +416,11 @@ static flow_t flow_at(const orc_params* P, const orc_medium* md, const double* x
     if (md->kind == M_GRID) {
         double o[3];
         grid_lookup(md, x[0], x[1], t, o);
-        /* the grid holds the spatial four-velocity (u^x, u^y): speed |u| / sqrt(1 + u^2) */
+        /* the grid holds the flow velocity (v^x, v^y), as the reference's (r, t) tables do */
         double u2 = o[1] * o[1] + o[2] * o[2];
         double u = sqrt(u2);
         if (u < ORC_EPS) return f;
-        f.v = u / sqrt(1.0 + u2); f.nx = o[1] / u; f.ny = o[2] / u; f.active = 1;
+        f.v = u; f.nx = o[1] / u; f.ny = o[2] / u; f.active = 1;
         return f;
     }
     /* kernels_cpu.jl:69-87 */
@@ -576,8 +576,7 @@ static void set_to_fluid(const orc_params* P, const orc_medium* md, const double
         double u = sqrt(o[1] * o[1] + o[2] * o[2]);
         if (u < ORC_EPS) { p[0] = 0.0; p[1] = 0.0; return; }
         double vmax = sqrt(1.0 - 1e-12);
-        double v = u / sqrt(1.0 + u * u);
-        double vc = P->relativistic ? jl_clamp(v, -vmax, vmax) : v;
+        double vc = P->relativistic ? jl_clamp(u, -vmax, vmax) : u;
         double g = P->relativistic ? 1.0 / sqrt(1.0 - vc * vc + 1e-10) : 1.0;
         p[0] = m * g * vc * (o[1] / u);
         p[1] = m * g * vc * (o[2] / u);
