@@ -269,6 +269,24 @@ int lim_adjoint(lim_ctx* ctx, int64_t first_step, int64_t nsteps, int64_t checkp
 /* Device time (ms) of the last lim_adjoint: checkpointed forward and reverse sweep. */
 int lim_adjoint_stats(lim_ctx* ctx, double* forward_ms, double* reverse_ms);
 
+/* ---- initial states -------------------------------------------------------------
+ * Samples n heavy quarks on the device from a FONLL-type density f(r, p) on an r grid
+ * (nr nodes) and a |p_T| grid (np nodes), f[ip + np*ir] = f(r_grid[ir], p_grid[ip])
+ * (Julia's Np x Nr matrix, column-major), into the context's state (replacing an
+ * uploaded one); then lim_initial_lab_boost / lim_run proceed as after lim_upload_state.
+ * Replaces sample_particles_from_FONLL (utils.jl:33-172): cartesian != 0 is its
+ * rejection sampling in (x, y) with |p| from the conditional inverse CDF of p | r,
+ * cartesian == 0 its polar mode (r from the r marginal, uniform angle); antithetic
+ * pairs (0,1), (2,3), ... share their draws, the second with -p.  thermal_pz != 0 (pdim
+ * 3) appends p_z from the local temperature of the context's medium at t0 as
+ * append_thermal_pz / sample_pz_conditional_juttner (utils.jl:499-551).  The draws come
+ * from the particle's Philox stream (seed, particle_offset + pair index, trial, tag),
+ * not a global RNG: the result depends on (seed, particle_offset) only.
+ * Needs Cartesian coordinates, dimensions 2 and pdim 2 or 3; a set medium when
+ * thermal_pz.  LIM_ERR_STATE when a particle found no accepted trial in 100000. */
+int lim_sample_fonll(lim_ctx* ctx, const double* r_grid, int64_t nr, const double* p_grid, int64_t np,
+                     const double* f, int64_t n, int cartesian, int antithetic, int thermal_pz);
+
 /* ---- batches ------------------------------------------------------------------
  * Many independent ensembles — each a configured context with its own particle
  * count, step range, mass, transport tables and medium — advanced together: every

@@ -96,6 +96,8 @@ _SIGS = {
     "lim_copy_rta_decisions": ([C.c_void_p, C.c_void_p], C.c_int),
     "lim_adjoint": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
     "lim_adjoint_stats": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_sample_fonll": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, _DP, C.c_int64, C.c_int, C.c_int, C.c_int],
+                         C.c_int),
     "lim_batch_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
     "lim_batch_destroy": ([C.c_void_p], C.c_int),
     "lim_batch_last_error": ([C.c_void_p], C.c_char_p),
@@ -257,6 +259,22 @@ class Engine:
         """Upload from flat Julia-layout buffers (e.g. pinned host memory)."""
         self._check(self.lib.lim_upload_state(self.ctx, _dptr(xbuf), int(self.params.dims), _dptr(pbuf),
                                               int(self.params.pdim), int(n)))
+        self.n = int(n)
+
+    def sample_fonll(self, r_grid, p_grid, f, n: int, *, cartesian: bool = True, antithetic: bool = False,
+                     thermal_pz: bool = False):
+        """Sample n initial particles on the device from the density f(r, p) (Julia's
+        shape (Np, Nr), as sample_particles_from_FONLL takes it) into the state."""
+        rg = np.ascontiguousarray(r_grid, dtype=np.float64)
+        pg = np.ascontiguousarray(p_grid, dtype=np.float64)
+        fm = np.asarray(f, dtype=np.float64)
+        if fm.shape != (pg.size, rg.size) and fm.shape == (rg.size, pg.size):
+            fm = fm.T                                   # Nr x Np is transposed, as utils.jl:43-49 does
+        if fm.shape != (pg.size, rg.size):
+            raise ValueError(f"f must have shape (len(p_grid), len(r_grid)) = {(pg.size, rg.size)}, got {fm.shape}")
+        fb = np.ascontiguousarray(fm.T).reshape(-1)
+        self._check(self.lib.lim_sample_fonll(self.ctx, _dptr(rg), rg.size, _dptr(pg), pg.size, _dptr(fb), int(n),
+                                              int(bool(cartesian)), int(bool(antithetic)), int(bool(thermal_pz))))
         self.n = int(n)
 
     def download_state(self):

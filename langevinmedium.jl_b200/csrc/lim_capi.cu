@@ -4,6 +4,7 @@
 // collision_mode, simulate_gpu_wrapper.jl:54-55; spline range, transport.jl:182-184).
 // No exception crosses the ABI: every entry point returns a status and keeps the
 // message for lim_last_error().
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -513,6 +514,37 @@ template int ctx_build_kparams<float>(lim_ctx*, KParams<float>&);
 
 }  // namespace lim
 
+namespace {
+
+template <typename R>
+int sample_impl(lim_ctx* c, const SampleTables& st_host, int64_t n)
+{
+    int rc;
+    if ((rc = alloc_state<R>(c, n))) return rc;
+    if ((rc = dev_alloc(c, c->d_stage_x, (size_t)std::max<int64_t>(n, 1) * c->dims * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_stage_p, (size_t)std::max<int64_t>(n, 1) * c->pdim * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_status, sizeof(unsigned long long)))) return rc;
+    LIM_CUDA(c, cudaMemsetAsync(c->d_status.p, 0xff, sizeof(unsigned long long), c->stream));
+    c->n = n;
+    c->state_prec = (int)c->P.precision;
+    c->have_state = true;                 // the kernel parameters need the state buffers
+    KParams<R> kp;
+    if ((rc = build_kparams<R>(c, kp))) { c->have_state = false; return rc; }
+    LIM_CUDA(c, cudaMemsetAsync(st_host.failed, 0, sizeof(unsigned long long), c->stream));
+    LIM_CUDA(c, launch_sample_fonll<R>(kp, st_host, c->stream));
+    unsigned long long failed = 0;
+    LIM_CUDA(c, cudaMemcpyAsync(&failed, st_host.failed, sizeof failed, cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (failed) {
+        c->have_state = false;
+        return fail(c, LIM_ERR_STATE, "lim_sample_fonll: %llu particles found no accepted trial in %d trials",
+                    failed, st_host.max_trials);
+    }
+    return LIM_OK;
+}
+
+}  // namespace
+
 // ===========================================================================
 // C-ABI
 // ===========================================================================
@@ -557,7 +589,7 @@ int lim_destroy(lim_ctx* c)
                       &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
-                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt };
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -587,7 +619,7 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
                             &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
-                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt };
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -784,6 +816,112 @@ int lim_upload_state(lim_ctx* c, const double* x, int64_t dims, const double* p,
     c->dims = (int)dims; c->pdim = (int)pdim;
     c->have_state = false;
     return c->P.precision == LIM_FP32 ? upload_state_impl<float>(c, x, p, n) : upload_state_impl<double>(c, x, p, n);
+}
+
+
+int lim_sample_fonll(lim_ctx* c, const double* r_grid, int64_t nr, const double* p_grid, int64_t np,
+                     const double* f, int64_t n, int cartesian, int antithetic, int thermal_pz)
+{
+    if (!c) return LIM_ERR_ARG;
+    ++c->gen;
+    int rc = state_rows_ok(c);
+    if (rc) return rc;
+    if (c->P.coords != LIM_COORDS_CARTESIAN || c->P.dims != 2 || (c->P.pdim != 2 && c->P.pdim != 3))
+        return fail(c, LIM_ERR_UNSUPPORTED, "lim_sample_fonll samples the transverse plane: dimensions=2, "
+                                             "momentum_dimensions 2 or 3, Cartesian coordinates");
+    if (n < 0 || n > (int64_t)UINT32_MAX) return fail(c, LIM_ERR_ARG, "lim_sample_fonll: particle count out of range");
+    if (!r_grid || !p_grid || !f || nr < 2 || np < 2 || nr > INT32_MAX || np > INT32_MAX ||
+        nr * np > (int64_t)1 << 31)
+        return fail(c, LIM_ERR_ARG, "lim_sample_fonll: need r and p grids of 2 to 2^31 nodes and the density table");
+    if (!ascending(r_grid, (size_t)nr) || !ascending(p_grid, (size_t)np))
+        return fail(c, LIM_ERR_ARG, "lim_sample_fonll: r_grid and p_grid must be strictly ascending");
+    if (c->P.pdim == 3 && thermal_pz && c->med_kind < 0)
+        return fail(c, LIM_ERR_STATE, "lim_sample_fonll: the thermal p_z needs the medium (set it first)");
+    // utils.jl:33-172, in FP64 on the host: f[ip + np*ir] is f(r_ir, p_ip) (an Np x Nr Matrix)
+    double dr = 0.0, dp = 0.0;
+    for (int64_t k = 1; k < nr; ++k) dr += r_grid[k] - r_grid[k - 1];
+    for (int64_t k = 1; k < np; ++k) dp += p_grid[k] - p_grid[k - 1];
+    dr /= (double)(nr - 1);
+    dp /= (double)(np - 1);
+    const double eps = 2.220446049250313e-16;
+    std::vector<double> cdf_p((size_t)(nr * np), 0.0), nsp((size_t)nr, 0.0), cdf_r((size_t)nr, 0.0);
+    std::vector<int> mass((size_t)nr, 0);
+    for (int64_t ir = 0; ir < nr; ++ir) {
+        double tot = 0.0;
+        for (int64_t ip = 0; ip < np; ++ip) tot += p_grid[ip] * f[ip + np * ir];
+        nsp[ir] = tot * dp;                                    // n(r) = int p f dp (Cartesian mode)
+        if (!(tot > 0)) continue;
+        mass[ir] = 1;
+        double* row = cdf_p.data() + (size_t)ir * np;
+        double acc = 0.0;
+        for (int64_t ip = 0; ip < np; ++ip) { acc += p_grid[ip] * f[ip + np * ir]; row[ip] = acc * dp; }
+        row[0] = 0.0;
+        for (int64_t k = 1; k < np; ++k) row[k] = std::max(row[k], row[k - 1] + eps);
+        const double last = row[np - 1];
+        for (int64_t k = 0; k < np; ++k) row[k] /= last;
+        row[np - 1] = 1.0;
+    }
+    double fmax = 0.0;
+    for (double v : nsp) fmax = std::max(fmax, v);
+    fmax += eps;
+    if (!cartesian) {                                          // polar: P(r, p) ~ r p f
+        double Z = 0.0;
+        for (int64_t ir = 0; ir < nr; ++ir)
+            for (int64_t ip = 0; ip < np; ++ip) Z += r_grid[ir] * p_grid[ip] * f[ip + np * ir];
+        Z *= dr * dp;
+        if (Z == 0.0) return fail(c, LIM_ERR_ARG, "Distribution normalization is zero.");
+        double acc = 0.0;
+        for (int64_t ir = 0; ir < nr; ++ir) {
+            double pr = 0.0;
+            for (int64_t ip = 0; ip < np; ++ip) pr += r_grid[ir] * p_grid[ip] * f[ip + np * ir] / Z;
+            acc += pr * dp;
+            cdf_r[ir] = acc * dr;
+        }
+        cdf_r[0] = 0.0;
+        for (int64_t k = 1; k < nr; ++k) cdf_r[k] = std::max(cdf_r[k], cdf_r[k - 1] + eps);
+        const double last = cdf_r[nr - 1];
+        for (int64_t k = 0; k < nr; ++k) cdf_r[k] /= last;
+        cdf_r[nr - 1] = 1.0;
+    }
+    // one device block: r grid, p grid, cdf_r, n(r), cdf_p, mass, failure count
+    const size_t doubles = (size_t)(nr + np + nr + nr + nr * np);
+    const size_t bytes = doubles * sizeof(double) + (size_t)nr * sizeof(int) + 64;
+    cudaSetDevice(c->device);
+    if ((rc = dev_alloc(c, c->d_sample, bytes))) return rc;
+    double* d = (double*)c->d_sample.p;
+    size_t off = 0;
+    auto put = [&](const double* src, size_t cnt) {
+        double* dst = d + off;
+        off += cnt;
+        return cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyHostToDevice, c->stream) == cudaSuccess ? dst : nullptr;
+    };
+    SampleTables st;
+    std::memset(&st, 0, sizeof st);
+    st.r_grid = put(r_grid, (size_t)nr);
+    st.p_grid = put(p_grid, (size_t)np);
+    st.cdf_r = put(cdf_r.data(), (size_t)nr);
+    st.n_spatial = put(nsp.data(), (size_t)nr);
+    st.cdf_p = put(cdf_p.data(), cdf_p.size());
+    if (!st.r_grid || !st.p_grid || !st.cdf_r || !st.n_spatial || !st.cdf_p)
+        return fail(c, LIM_ERR_CUDA, "lim_sample_fonll: table upload failed");
+    int* dm = (int*)(d + off);
+    LIM_CUDA(c, cudaMemcpyAsync(dm, mass.data(), mass.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    st.p_mass = dm;
+    st.failed = (unsigned long long*)(((uintptr_t)(dm + nr) + 15) & ~(uintptr_t)15);
+    st.nr = (int)nr; st.np = (int)np;
+    st.f_max = fmax;
+    st.rmax = r_grid[nr - 1];
+    st.cartesian = cartesian != 0;
+    st.antithetic = antithetic != 0;
+    st.with_pz = thermal_pz != 0;
+    st.med_kind = c->med_kind;
+    st.max_trials = 100000;
+    c->dims = 2;
+    c->pdim = (int)c->P.pdim;
+    c->have_state = false;
+    rc = c->P.precision == LIM_FP32 ? sample_impl<float>(c, st, n) : sample_impl<double>(c, st, n);
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));    // the host tables are released on return
+    return rc;
 }
 
 int lim_download_state(lim_ctx* c, double* x, double* p)

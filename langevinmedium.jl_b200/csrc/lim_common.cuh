@@ -11,7 +11,8 @@ constexpr double kEps = 2.220446049250313e-16;   // Julia eps()
 constexpr double kFmGeV = 1.0 / 0.197327;        // constants.jl:13,23
 constexpr int kNoiseSlots = 11;
 constexpr int kTapeFields = 8;   // adjoint tape per step: two float4, (x0, x1, p0, p1) and (p2, xi0, xi1, xi2)
-enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4 };
+enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4,
+       TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6, TAG_SAMPLE_PZ = 7 };   // initial-state sampling (lim_sample.cu)
 enum { MED_RT = 0, MED_BJORKEN = 1, MED_GRID = 2 };
 enum { COLL_LANGEVIN = 0, COLL_RTA = 1, COLL_LANGEVIN_RTA = 2, COLL_FLUID = 3 };
 

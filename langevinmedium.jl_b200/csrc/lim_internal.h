@@ -81,6 +81,22 @@ cudaError_t launch_adjoint_tape(const KParams<float>& kp, int64_t s0, int64_t s1
 cudaError_t launch_adjoint_rev(const KParams<float>& kp, const AdjointArgs& aa, int64_t s0, int64_t s1, cudaStream_t st);
 cudaError_t launch_adjoint_total(const KParams<float>& kp, const AdjointArgs& aa, double* out, cudaStream_t st);
 
+// Initial-state sampling (lim_sample.cu) from the tables of sample_particles_from_FONLL
+// (utils.jl:33-172), built on the host in FP64.
+struct SampleTables {
+    const double* r_grid; int nr;
+    const double* p_grid; int np;
+    const double* cdf_r;         // nr: CDF of the r marginal (polar mode)
+    const double* cdf_p;         // nr x np: row j is the CDF of |p| given r_j
+    const int* p_mass;           // nr: row j has non-zero mass
+    const double* n_spatial;     // nr: spatial density (Cartesian mode)
+    double f_max, rmax;
+    int cartesian, antithetic, with_pz, med_kind, max_trials;
+    unsigned long long* failed;  // particles without an accepted trial
+};
+template <typename R>
+cudaError_t launch_sample_fonll(const KParams<R>& kp, const SampleTables& st, cudaStream_t s);
+
 cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
 
 // FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.

@@ -112,33 +112,42 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
     Vfield = np.asarray(VelocityEvolutionn, dtype=np.float64)
     rng = np.random.default_rng(int(seed) & 0xFFFFFFFFFFFFFFFF)
     # --- initial state (simulate_cpu.jl:63-94) ---
-    if x_init is None or p_init is None:
-        raise NotImplementedError("the B200 backend takes the initial state from x_init/p_init; "
-                                  "sample it with the reference's samplers (utils.jl) and pass it in")
-    x_matrix = np.array(x_init, dtype=np.float64, ndmin=2)
-    p_matrix = np.array(p_init, dtype=np.float64, ndmin=2)
-    radial_mode = dimensions == 1
-    if radial_mode:
-        if x_matrix.shape[0] >= 2:
-            positions, momenta = radial_reduction(x_matrix[:2], p_matrix[:2], r_grid_Langevin, rng)
-        else:
-            positions, momenta = x_matrix, p_matrix
-    else:
-        positions, momenta = x_matrix.copy(), p_matrix.copy()
     pdim = dimensions if momentum_dimensions <= 0 else momentum_dimensions
-    check_momentum_dims(dimensions, pdim, radial_mode, bjorken_redshift, initial_time)
-    if momenta.shape[0] < pdim:
+    device_sampling = x_init is None or p_init is None
+    if device_sampling:
+        # sample_particles_from_FONLL (utils.jl:33-172) on the device, with the thermal p_z
+        # of append_thermal_pz (utils.jl:533-551) from the medium at initial_time
+        if dimensions != 2:
+            raise NotImplementedError("the B200 backend samples the FONLL initial state on the device for "
+                                      "dimensions=2; for dimensions 1 and 3 pass x_init/p_init")
+        check_momentum_dims(dimensions, pdim, False, bjorken_redshift, initial_time)
+        do_cartesian = True if cartesian_spatial_sampling is None else bool(cartesian_spatial_sampling)
+        N = int(N_particles)
+    else:
+        x_matrix = np.array(x_init, dtype=np.float64, ndmin=2)
+        p_matrix = np.array(p_init, dtype=np.float64, ndmin=2)
+        radial_mode = dimensions == 1
+        if radial_mode:
+            if x_matrix.shape[0] >= 2:
+                positions, momenta = radial_reduction(x_matrix[:2], p_matrix[:2], r_grid_Langevin, rng)
+            else:
+                positions, momenta = x_matrix, p_matrix
+        else:
+            positions, momenta = x_matrix.copy(), p_matrix.copy()
+        check_momentum_dims(dimensions, pdim, radial_mode, bjorken_redshift, initial_time)
+    if not device_sampling and momenta.shape[0] < pdim:
         from .utils import _rt_interp_host
         momenta = append_thermal_pz(momenta, positions, m,
                                     lambda r: _rt_interp_host(xgrid, tgrid, Tfield, r, initial_time),
                                     antithetic=antithetic_momenta and x_init is None, rng=rng)
-    if momenta.shape[0] != pdim:
-        raise ValueError(f"momentum rows {momenta.shape[0]} ≠ momentum_dimensions {pdim}")
-    if positions.shape[0] != dimensions:
-        raise ValueError(f"position rows {positions.shape[0]} ≠ dimensions {dimensions}")
-    N = positions.shape[1]
-    if momenta.shape[1] != N:
-        raise ValueError("x_init and p_init hold different particle counts")
+    if not device_sampling:
+        if momenta.shape[0] != pdim:
+            raise ValueError(f"momentum rows {momenta.shape[0]} ≠ momentum_dimensions {pdim}")
+        if positions.shape[0] != dimensions:
+            raise ValueError(f"position rows {positions.shape[0]} ≠ dimensions {dimensions}")
+        N = positions.shape[1]
+        if momenta.shape[1] != N:
+            raise ValueError("x_init and p_init hold different particle counts")
 
     # --- engine configuration ---
     if not momentum_langevin or DsT == 0.0:
@@ -176,7 +185,11 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
             eng.set_invcdf(inv, nU, nT, Ttmin, Tinv)
     elif mode in ("rta", "langevin_rta"):
         eng.set_invcdf(np.zeros(4), 2, 2, 0.0, 1.0)   # reference default table (simulate_gpu.jl:124-128)
-    eng.upload_state(positions, momenta)
+    if device_sampling:
+        eng.sample_fonll(r_grid_Langevin, p_grid_Langevin, heavy_quark_density, N, cartesian=do_cartesian,
+                         antithetic=antithetic_momenta, thermal_pz=pdim == 3)
+    else:
+        eng.upload_state(positions, momenta)
     eng.initial_lab_boost()
 
     if freezeout_capture:

@@ -33,7 +33,8 @@
 
 enum { C_LANGEVIN = 0, C_RTA = 1, C_LANGEVIN_RTA = 2, C_FLUID = 3 };
 enum { M_RT = 0, M_BJORKEN = 1, M_GRID = 2 };
-enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4 };
+enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4, TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6,
+       TAG_SAMPLE_PZ = 7 };
 
 typedef struct orc_params {
     double dt, t0, m, DsT, Tfo, psi2, obs_pt_cut, obs_pt_width;
@@ -865,4 +866,185 @@ int orc_max_threads(void)
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------- */
+/* Initial-state sampling (checker of lim_sample_fonll)                       */
+/* ------------------------------------------------------------------------- */
+/* utils.jl:33-172 sample_particles_from_FONLL and utils.jl:499-551
+ * sample_pz_conditional_juttner / append_thermal_pz, drawing from the particle's
+ * counter-based stream instead of the global RNG: block (pid, trial, tag). */
+static int64_t ss_last(const double* g, int64_t n, double x)   /* searchsortedlast, 0-based, capped to n-2 */
+{
+    int64_t lo = -1, hi = n;
+    while (hi - lo > 1) { int64_t mid = (lo + hi) / 2; if (g[mid] <= x) lo = mid; else hi = mid; }
+    if (lo < 0) lo = 0;
+    return lo > n - 2 ? n - 2 : lo;
+}
+static double inv_cdf(const double* cdf, const double* grid, int64_t n, double u)
+{
+    if (u <= cdf[0]) return grid[0];
+    if (u >= cdf[n - 1]) return grid[n - 1];
+    int64_t k = ss_last(cdf, n, u);
+    double w = (u - cdf[k]) / (cdf[k + 1] - cdf[k]);
+    return grid[k] + w * (grid[k + 1] - grid[k]);
+}
+static void words(const orc_params* P, int64_t pid, int64_t draw, int tag, uint32_t w[4])
+{
+    uint32_t key[2] = { (uint32_t)(uint64_t)P->seed, (uint32_t)((uint64_t)P->seed >> 32) };
+    uint32_t ctr[4] = { (uint32_t)pid, (uint32_t)draw, (uint32_t)tag, 0u };
+    orc_philox4x32_10(ctr, key, w);
+}
+static double sample_pz_cond(const orc_params* P, int64_t pid, double mT, double T, int max_trials)
+{
+    if (!(T > 0.0 && mT > 0.0)) return 0.0;
+    double a = mT / T;
+    if (a > 1.05) {
+        double c = a / (a - 1.0) > 2.0 ? a / (a - 1.0) : 2.0;
+        double sig = sqrt(c / a);
+        for (int t = 0; t < max_trials; ++t) {
+            uint32_t w[4];
+            double z0, z1;
+            words(P, pid, t, TAG_SAMPLE_PZ, w);
+            box_muller(u01(w[0]), u01(w[1]), &z0, &z1);
+            double y = sig * z0, ch = cosh(y);
+            double acc = ch * exp(-a * (ch - 1.0) + a * y * y / (2.0 * c));
+            if (u01(w[2]) <= acc) return mT * sinh(y);
+        }
+        return 0.0;
+    }
+    double b = sqrt(2.0) * T;
+    for (int t = 0; t < 10 * max_trials; ++t) {           /* 1e6 trials for the loose envelope */
+        uint32_t w[4];
+        words(P, pid, t, TAG_SAMPLE_PZ, w);
+        double pz = -b * log(u01(w[0])) * (u01(w[1]) < 0.5 ? -1.0 : 1.0);
+        double acc = exp(-(sqrt(mT * mT + pz * pz) - (mT + fabs(pz)) / sqrt(2.0)) / T);
+        if (u01(w[2]) <= acc) return pz;
+    }
+    return 0.0;
+}
+
+/* p_z draws of particles pid = particle_offset + 0 .. n-1 at fixed (mT, T). */
+void orc_sample_pz(const orc_params* P, double mT, double T, int64_t n, double* out)
+{
+    for (int64_t i = 0; i < n; ++i) out[i] = sample_pz_cond(P, P->particle_offset + i, mT, T, 100000);
+}
+
+/* Samples n particles into x (2, n) and p (pdim, n), column-major (Julia) layout.
+ * f[ip + np*ir] = f(r_ir, p_ip).  Returns the number of particles without an accepted
+ * trial, or -1 when the polar normalisation is zero. */
+int64_t orc_sample_fonll(const orc_params* P, const orc_medium* md, const double* r_grid, int64_t nr,
+                         const double* p_grid, int64_t np, const double* f, int64_t n, int cartesian,
+                         int antithetic, int thermal_pz, double* x, double* p)
+{
+    const double eps = 2.220446049250313e-16;
+    const int max_trials = 100000;
+    double dr = 0.0, dp = 0.0;
+    for (int64_t k = 1; k < nr; ++k) dr += r_grid[k] - r_grid[k - 1];
+    for (int64_t k = 1; k < np; ++k) dp += p_grid[k] - p_grid[k - 1];
+    dr /= (double)(nr - 1);
+    dp /= (double)(np - 1);
+    double* cdf_p = calloc((size_t)(nr * np), sizeof(double));
+    double* nsp = calloc((size_t)nr, sizeof(double));
+    double* cdf_r = calloc((size_t)nr, sizeof(double));
+    int* mass = calloc((size_t)nr, sizeof(int));
+    for (int64_t ir = 0; ir < nr; ++ir) {
+        double tot = 0.0;
+        for (int64_t ip = 0; ip < np; ++ip) tot += p_grid[ip] * f[ip + np * ir];
+        nsp[ir] = tot * dp;
+        if (!(tot > 0)) continue;
+        mass[ir] = 1;
+        double* row = cdf_p + ir * np, acc = 0.0;
+        for (int64_t ip = 0; ip < np; ++ip) { acc += p_grid[ip] * f[ip + np * ir]; row[ip] = acc * dp; }
+        row[0] = 0.0;
+        for (int64_t k = 1; k < np; ++k) row[k] = jl_max(row[k], row[k - 1] + eps);
+        double last = row[np - 1];
+        for (int64_t k = 0; k < np; ++k) row[k] /= last;
+        row[np - 1] = 1.0;
+    }
+    double fmax = 0.0;
+    for (int64_t k = 0; k < nr; ++k) fmax = jl_max(fmax, nsp[k]);
+    fmax += eps;
+    int64_t failed = 0;
+    if (!cartesian) {
+        double Z = 0.0;
+        for (int64_t ir = 0; ir < nr; ++ir)
+            for (int64_t ip = 0; ip < np; ++ip) Z += r_grid[ir] * p_grid[ip] * f[ip + np * ir];
+        Z *= dr * dp;
+        if (Z == 0.0) { failed = -1; goto done; }
+        double acc = 0.0;
+        for (int64_t ir = 0; ir < nr; ++ir) {
+            double pr = 0.0;
+            for (int64_t ip = 0; ip < np; ++ip) pr += r_grid[ir] * p_grid[ip] * f[ip + np * ir] / Z;
+            acc += pr * dp;
+            cdf_r[ir] = acc * dr;
+        }
+        cdf_r[0] = 0.0;
+        for (int64_t k = 1; k < nr; ++k) cdf_r[k] = jl_max(cdf_r[k], cdf_r[k - 1] + eps);
+        double last = cdf_r[nr - 1];
+        for (int64_t k = 0; k < nr; ++k) cdf_r[k] /= last;
+        cdf_r[nr - 1] = 1.0;
+    }
+    {
+        const double rmax = r_grid[nr - 1];
+        const int64_t half = n / 2;
+        for (int64_t i = 0; i < n; ++i) {
+            int64_t draw = i;
+            int mirror = 0;
+            if (antithetic) {
+                if (i < 2 * half) { draw = i / 2; mirror = (int)(i & 1); }
+                else draw = half;
+            }
+            const int64_t pid = P->particle_offset + draw;
+            double xx = 0.0, yy = 0.0, r = 0.0, pm = 0.0, php = 0.0;
+            uint32_t w[4], v[4];
+            if (cartesian) {
+                int ok = 0;
+                for (int t = 0; t < max_trials && !ok; ++t) {
+                    words(P, pid, t, TAG_SAMPLE_XY, w);
+                    double xt = rmax * (2.0 * u01(w[0]) - 1.0), yt = rmax * (2.0 * u01(w[1]) - 1.0);
+                    double rt = sqrt(xt * xt + yt * yt);
+                    if (rt > rmax) continue;
+                    double nrv = 0.0;
+                    if (rt >= r_grid[0] && rt <= r_grid[nr - 1]) {
+                        int64_t k = ss_last(r_grid, nr, rt);
+                        double wk = (rt - r_grid[k]) / (r_grid[k + 1] - r_grid[k]);
+                        nrv = nsp[k] + wk * (nsp[k + 1] - nsp[k]);
+                    }
+                    if (u01(w[2]) * fmax > nrv) continue;
+                    xx = xt; yy = yt; r = rt;
+                    words(P, pid, t, TAG_SAMPLE_P, v);
+                    double rc = jl_clamp(r, r_grid[0], r_grid[nr - 1]);
+                    int64_t j = ss_last(r_grid, nr, rc) + (rc >= r_grid[nr - 1] ? 1 : 0);
+                    pm = mass[j] ? inv_cdf(cdf_p + j * np, p_grid, np, u01(v[0])) : 0.0;
+                    php = 2.0 * M_PI * u01(v[1]);
+                    ok = 1;
+                }
+                if (!ok) ++failed;
+            } else {
+                words(P, pid, 0, TAG_SAMPLE_XY, w);
+                r = jl_clamp(inv_cdf(cdf_r, r_grid, nr, u01(w[0])), r_grid[0], r_grid[nr - 1]);
+                double phi = 2.0 * M_PI * u01(w[1]);
+                xx = r * cos(phi); yy = r * sin(phi);
+                int64_t j = ss_last(r_grid, nr, r) + (r >= r_grid[nr - 1] ? 1 : 0);
+                pm = mass[j] ? inv_cdf(cdf_p + j * np, p_grid, np, u01(w[2])) : 0.0;
+                php = 2.0 * M_PI * u01(w[3]);
+            }
+            double px = pm * cos(php), py = pm * sin(php), pz = 0.0;
+            if (P->pdim == 3 && thermal_pz) {
+                double xv[3] = { xx, yy, 0.0 };
+                double T = medium_T(md, xv, sqrt(xx * xx + yy * yy), P->t0);
+                T = T > 0.0 ? T : 0.0;
+                double mT = sqrt(P->m * P->m + px * px + py * py);
+                pz = sample_pz_cond(P, pid, mT, T, max_trials);
+            }
+            if (mirror) { px = -px; py = -py; pz = -pz; }
+            x[2 * i] = xx; x[2 * i + 1] = yy;
+            p[P->pdim * i] = px; p[P->pdim * i + 1] = py;
+            if (P->pdim == 3) p[P->pdim * i + 2] = pz;
+        }
+    }
+done:
+    free(cdf_p); free(nsp); free(cdf_r); free(mass);
+    return failed;
 }

@@ -83,6 +83,11 @@ def lib() -> C.CDLL:
         L.orc_max_threads.restype = C.c_int
         L.orc_step_variates.argtypes = [C.POINTER(OrcParams), C.c_int64, C.c_int64, C.c_int, _DP]
         L.orc_step_variates.restype = None
+        L.orc_sample_fonll.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcMedium), _DP, C.c_int64, _DP, C.c_int64,
+                                       _DP, C.c_int64, C.c_int, C.c_int, C.c_int, _DP, _DP]
+        L.orc_sample_fonll.restype = C.c_int64
+        L.orc_sample_pz.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, _DP]
+        L.orc_sample_pz.restype = None
         assert L.orc_sizeof_params() == C.sizeof(OrcParams)
         assert L.orc_sizeof_medium() == C.sizeof(OrcMedium)
         assert L.orc_sizeof_fo() == FO_FIELDS * 8
@@ -239,3 +244,27 @@ def step_variates(P, pid, step, kick=True):
 
 def max_threads() -> int:
     return int(lib().orc_max_threads())
+
+
+def sample_fonll(P: OrcParams, md: Medium | None, r_grid, p_grid, f, n, *, cartesian=True, antithetic=False,
+                 thermal_pz=False):
+    """Restatement of the device FONLL sampler.  f has Julia's shape (Np, Nr).
+    Returns (x (2, n), p (pdim, n), failed)."""
+    rg = np.ascontiguousarray(r_grid, dtype=np.float64)
+    pg = np.ascontiguousarray(p_grid, dtype=np.float64)
+    fm = np.asarray(f, dtype=np.float64)
+    assert fm.shape == (pg.size, rg.size)
+    fb = np.ascontiguousarray(fm.T).reshape(-1)          # f[ip + np*ir]
+    xb = np.zeros(max(2 * n, 1))
+    pb = np.zeros(max(P.pdim * n, 1))
+    mds = None if md is None else C.byref(md.s)
+    failed = lib().orc_sample_fonll(C.byref(P), mds, _d(rg), rg.size, _d(pg), pg.size, _d(fb), int(n),
+                                    int(bool(cartesian)), int(bool(antithetic)), int(bool(thermal_pz)), _d(xb), _d(pb))
+    return from_flat(xb[:2 * n], 2, n), from_flat(pb[:P.pdim * n], P.pdim, n), int(failed)
+
+
+def sample_pz(P: OrcParams, mT, T, n):
+    """p_z draws of particles particle_offset + 0 .. n-1 at fixed (mT, T)."""
+    out = np.zeros(max(int(n), 1))
+    lib().orc_sample_pz(C.byref(P), float(mT), float(T), int(n), _d(out))
+    return out[:int(n)]
