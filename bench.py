@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import math
 import os
 import statistics
@@ -178,13 +179,13 @@ def work_model(pkg):
 
 
 def traffic_from_profile():
-    p = ROOT / "profiles" / "k_cart_bjorken_fp32_traffic.json"
+    """dram__bytes_read + dram__bytes_write of one benchmark launch, from the committed
+    ncu summary of the step kernel (its last line)."""
+    p = ROOT / "profiles" / "k_cart_bjorken_fp32_traffic.md"
     if p.exists():
-        try:
-            d = json.loads(p.read_text())
-            return d.get("bytes_per_launch_full_size")
-        except (ValueError, KeyError):
-            return None
+        m = re.search(r"^bytes_per_launch_full_size:\s*(\d+)\s*$", p.read_text(), re.M)
+        if m:
+            return int(m.group(1))
     return None
 
 
