@@ -2,10 +2,12 @@
 // observables with respect to the drag parametrisation (a, b) of D_s(T) and the
 // medium temperature scale s, with the noise and the RTA indicators held fixed.
 //
-// The forward pass checkpoints the state every K steps.  The reverse sweep then takes
-// the segments from the last: k_tape recomputes a segment from its checkpoint with
-// the primal step (RTA decisions replayed from the forward pass's record), writing the
-// pre-step state and the momentum normals of every step to a tape; k_adjoint_rev walks
+// The forward pass checkpoints the state every K steps and tapes the last segment.
+// The reverse sweep then takes the segments from the last: k_tape recomputes a segment
+// from its checkpoint with the primal step (RTA decisions replayed from the forward
+// pass's record), writing to a tape what the reverse step needs: the pre-step momentum,
+// the momentum normals and, on the 2+1D grid, the medium the step saw with its
+// gradient (so the reverse needs no grid lookups); k_adjoint_rev walks
 // the segment backwards, applying the hand-derived vector-Jacobian product of each step
 // to two cotangents carried between segments in HBM.  All three observables are
 // functions of the final (p_x, p_y), so the cotangents start as the unit vectors of
@@ -21,7 +23,7 @@
 // lim_step.cuh (its frame change is this map, up to the reference's 1e-10 under the
 // square root of gamma), smooth in V at V = 0; the cotangent of u maps back to the
 // velocity field through du/dV = g I + g^3 V V^T.
-// Intermediates are re-evaluated in FP32 from the taped state; slopes of the
+// Intermediates are re-evaluated in FP32 from the taped values; slopes of the
 // tabulated functions come from tables differenced in FP64 on the host.
 #include "lim_internal.h"
 #include "lim_particle.cuh"
@@ -29,39 +31,6 @@
 namespace lim {
 
 namespace {
-
-// Trilinear (T, v^x, v^y) at (x, y) and their gradients in x and y (zero along an
-// axis where the query is clamped to the grid).
-__device__ __forceinline__ void grid_lookup_grad(const MediumDev<float>& md, const StepRec<float>& sr, float xq, float yq,
-                                                 float& T, float& ux, float& uy, float (&dT)[2], float (&dux)[2],
-                                                 float (&duy)[2])
-{
-    int ix, iy;
-    float wx, wy;
-    grid_cell(md, xq, yq, ix, iy, wx, wy);
-    const float kx = (xq > (float)md.gx0_d && xq < (float)md.gxl_d) ? md.ginvdx : 0.0f;
-    const float ky = (yq > (float)md.gy0_d && yq < (float)md.gyl_d) ? md.ginvdy : 0.0f;
-    const float wt = sr.wt;
-    const float4* s0 = md.G + ((size_t)sr.kt * md.gny + iy) * md.gnx + ix;
-    const float4* s1 = s0 + (size_t)md.gny * md.gnx;
-    const float4 a00 = __ldg(s0), a10 = __ldg(s0 + 1), a01 = __ldg(s0 + md.gnx), a11 = __ldg(s0 + md.gnx + 1);
-    const float4 b00 = __ldg(s1), b10 = __ldg(s1 + 1), b01 = __ldg(s1 + md.gnx), b11 = __ldg(s1 + md.gnx + 1);
-    // per component: value and d/dwx, d/dwy of the time-interpolated bilinear
-    auto tri = [&](float A00, float A10, float A01, float A11, float B00, float B10, float B01, float B11,
-                   float& v, float& gx, float& gy) {
-        const float r0a = A00 + wx * (A10 - A00), r1a = A01 + wx * (A11 - A01);
-        const float r0b = B00 + wx * (B10 - B00), r1b = B01 + wx * (B11 - B01);
-        const float va = r0a + wy * (r1a - r0a), vb = r0b + wy * (r1b - r0b);
-        v = va + wt * (vb - va);
-        const float gxa = (A10 - A00) + wy * ((A11 - A01) - (A10 - A00));
-        const float gxb = (B10 - B00) + wy * ((B11 - B01) - (B10 - B00));
-        gx = (gxa + wt * (gxb - gxa)) * kx;
-        gy = ((r1a - r0a) + wt * ((r1b - r0b) - (r1a - r0a))) * ky;
-    };
-    tri(a00.x, a10.x, a01.x, a11.x, b00.x, b10.x, b01.x, b11.x, T, dT[0], dT[1]);
-    tri(a00.y, a10.y, a01.y, a11.y, b00.y, b10.y, b01.y, b11.y, ux, dux[0], dux[1]);
-    tri(a00.z, a10.z, a01.z, a11.z, b00.z, b10.z, b01.z, b11.z, uy, duy[0], duy[1]);
-}
 
 // The Jüttner inverse CDF at (word w, T) as invcdf_lookup computes it, with its
 // derivative in T (zero where the T weight is clamped).
@@ -123,19 +92,19 @@ __device__ __forceinline__ void boost_fwd(float sg, const float (&p)[3], float m
 
 // The reverse of step s for NC cotangents: lx, lp (of the post-step state) become
 // those of the pre-step state (xs, ps); g[o][k] accumulates the parameter part.
+// mg: the medium the step saw (from the tape; T only for Bjorken); zf: the step's
+// Bjorken redshift factor of p_z.
 template <int MED, int NC>
-__device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const StepRec<float>& sr, int64_t s, int64_t i,
-                                             const NoiseKey& nk, const float (&xs)[2], const float (&ps)[3],
-                                             const float (&xi)[3], float (&lx)[NC][2], float (&lp)[NC][3],
-                                             float (&g)[NC][3])
+__device__ __forceinline__ void adjoint_step(const KParams<float>& kp, int64_t s, int64_t i, const NoiseKey& nk,
+                                             const MedGrad& mg, float zf, const float (&ps)[3], const float (&xi)[3],
+                                             float (&lx)[NC][2], float (&lp)[NC][3], float (&g)[NC][3])
 {
     const float m = kp.m, dt = kp.dtR;
     // ---- A. medium
-    float Tf, ux = 0.0f, uy = 0.0f;
-    float dT[2] = { 0.0f, 0.0f }, dux[2] = { 0.0f, 0.0f }, duy[2] = { 0.0f, 0.0f };
-    float vx = 0.0f, vy = 0.0f;                 // the grid's flow velocity
-    if (MED == MED_GRID) grid_lookup_grad(kp.med, sr, xs[0], xs[1], Tf, vx, vy, dT, dux, duy);
-    else Tf = sr.T_bj;
+    float ux = 0.0f, uy = 0.0f;
+    const float Tf = mg.T;
+    const float vx = MED == MED_GRID ? mg.vx : 0.0f, vy = MED == MED_GRID ? mg.vy : 0.0f;
+    const float dT[2] = { mg.dT[0], mg.dT[1] }, dux[2] = { mg.dvx[0], mg.dvx[1] }, duy[2] = { mg.dvy[0], mg.dvy[1] };
     const float sc = kp.med.T_scale;
     const float T = Tf * sc;
     const bool flow = MED == MED_GRID && !(sqrtf(vx * vx + vy * vy) < (float)kEps);
@@ -148,7 +117,6 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, const Ste
     else { p1[0] = ps[0]; p1[1] = ps[1]; p1[2] = ps[2]; }
     // ---- C. redshift
     float p2[3] = { p1[0], p1[1], p1[2] };
-    const float zf = (float)sr.zf;
     if (kp.redshift) p2[2] *= zf;
     // ---- D. kick
     const float Tk = jmax0(T);
@@ -286,7 +254,7 @@ __device__ __forceinline__ void final_observables(double px, double py, double c
 
 // Recomputes steps [s0, s1) from the checkpoint the parameters point at, taping them.
 template <int MED>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_tape(const KParams<float> kp, int64_t s0, int64_t s1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -332,14 +300,34 @@ k_adjoint_rev(const KParams<float> kp, const AdjointArgs aa, int64_t s0, int64_t
     }
     const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<float>* __restrict__ tab = (const StepRec<float>*)kp.steps - kp.step_base;
-    const float4* t = reinterpret_cast<const float4*>(kp.tape) + (size_t)(s1 - 1 - s0) * 2 * n + i;
-    for (int64_t s = s1 - 1; s >= s0; --s, t -= 2 * n) {
-        const float4 ta = __ldg(t), tb = __ldg(t + n);
-        const float xs[2] = { ta.x, ta.y };
-        const float ps[3] = { ta.z, ta.w, tb.x };
-        const float xi[3] = { tb.y, tb.z, tb.w };
-        const StepRec<float> sr = tab[s];
-        adjoint_step<MED, kAdjCot>(kp, sr, s, i, nk, xs, ps, xi, lx, lp, g);
+    constexpr int rows = tape_rows(MED);
+    const float4* t = reinterpret_cast<const float4*>(kp.tape) + (size_t)(s1 - 1 - s0) * rows * n + i;
+    // the next (earlier) step's first two rows are loaded while the current step is
+    // differentiated
+    float4 na = __ldg(t), nb = __ldg(t + n);
+    for (int64_t s = s1 - 1; s >= s0; --s) {
+        const float4 ta = na, tb = nb;
+        MedGrad mg;
+        float ps[3];
+        if (MED == MED_GRID) {
+            const float4 tc = __ldg(t + 2 * n), td = __ldg(t + 3 * n);
+            ps[0] = ta.x; ps[1] = ta.y; ps[2] = ta.z;
+            mg.T = ta.w; mg.vx = tb.w; mg.vy = tc.x;
+            mg.dT[0] = tc.y; mg.dT[1] = tc.z; mg.dvx[0] = tc.w;
+            mg.dvx[1] = td.x; mg.dvy[0] = td.y; mg.dvy[1] = td.z;
+        } else {
+            ps[0] = ta.z; ps[1] = ta.w; ps[2] = tb.x;
+            mg.T = tab[s].T_bj; mg.vx = mg.vy = 0.0f;
+            mg.dT[0] = mg.dT[1] = mg.dvx[0] = mg.dvx[1] = mg.dvy[0] = mg.dvy[1] = 0.0f;
+        }
+        const float xib[3] = { MED == MED_GRID ? tb.x : tb.y, MED == MED_GRID ? tb.y : tb.z,
+                               MED == MED_GRID ? tb.z : tb.w };
+        if (s > s0) {
+            t -= (size_t)rows * n;
+            na = __ldg(t);
+            nb = __ldg(t + n);
+        }
+        adjoint_step<MED, kAdjCot>(kp, s, i, nk, mg, (float)tab[s].zf, ps, xib, lx, lp, g);
     }
 #pragma unroll
     for (int o = 0; o < kAdjCot; ++o) {

@@ -61,7 +61,8 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
     const size_t seg_bytes = (size_t)n * (4 * sizeof(float) + 3 * sizeof(double));
     const size_t nn = (size_t)std::max<int64_t>(n, 1);
     if ((rc = ctx_alloc(c, c->d_adj_ckpt, std::max<size_t>(seg_bytes * (size_t)nseg, 16)))) return rc;
-    if ((rc = ctx_alloc(c, c->d_adj_tape, (size_t)std::min(K, nsteps) * kTapeFields * nn * sizeof(float)))) return rc;
+    if ((rc = ctx_alloc(c, c->d_adj_tape, (size_t)std::min(K, nsteps) * tape_rows(c->med_kind) * nn * sizeof(float4))))
+        return rc;
     if ((rc = ctx_alloc(c, c->d_adj_table, (size_t)nsteps * step_record_bytes<float>()))) return rc;
     const int64_t nblocks = std::max<int64_t>((n + kAdjBlock - 1) / kAdjBlock, 1);
     if ((rc = ctx_alloc(c, c->d_adj_part, (size_t)nblocks * kAdjOut * sizeof(double)))) return rc;
@@ -107,9 +108,18 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
     LIM_ACUDA(c, cudaEventRecord(e0, c->stream));
     // forward: checkpoint, then the segment's steps (one launch per segment: measured
     // faster than one launch that checkpoints from inside, whose extra live values cost
-    // occupancy)
+    // occupancy).  The last segment, the first one the reverse sweep needs, is taped
+    // directly instead of checkpointed and recomputed.
     const size_t fb = (size_t)n * sizeof(float), db = (size_t)n * sizeof(double);
     for (int64_t seg = 0; seg < nseg; ++seg) {
+        if (seg == nseg - 1) {
+            const int64_t s0 = first_step + seg * K, s1 = first_step + nsteps;
+            KParams<float> kt = kp;
+            kt.tape = (float*)c->d_adj_tape.p;
+            kt.tape_first = s0;
+            LIM_ACUDA(c, launch_adjoint_tape(kt, s0, s1, c->stream));
+            break;
+        }
         char* cb = (char*)c->d_adj_ckpt.p + (size_t)seg * seg_bytes;
         for (int d = 0; d < 2; ++d) {
             LIM_ACUDA(c, cudaMemcpyAsync(cb + d * fb, kp.x[d], fb, cudaMemcpyDeviceToDevice, c->stream));
@@ -142,7 +152,7 @@ int lim_adjoint(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t checkpoi
         for (int d = 0; d < 3; ++d) kq.p[d] = (double*)(cb + 4 * fb + d * db);
         const int64_t s0 = first_step + seg * K, s1 = std::min(s0 + K, first_step + nsteps);
         kq.tape_first = s0;
-        LIM_ACUDA(c, launch_adjoint_tape(kq, s0, s1, c->stream));
+        if (seg < nseg - 1) LIM_ACUDA(c, launch_adjoint_tape(kq, s0, s1, c->stream));
         LIM_ACUDA(c, launch_adjoint_rev(kq, aa, s0, s1, c->stream));
     }
     LIM_ACUDA(c, launch_adjoint_total(kp, aa, (double*)c->d_adj_out.p, c->stream));

@@ -10,10 +10,17 @@ namespace lim {
 constexpr double kEps = 2.220446049250313e-16;   // Julia eps()
 constexpr double kFmGeV = 1.0 / 0.197327;        // constants.jl:13,23
 constexpr int kNoiseSlots = 11;
-constexpr int kTapeFields = 8;   // adjoint tape per step: two float4, (x0, x1, p0, p1) and (p2, xi0, xi1, xi2)
 enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4,
        TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6, TAG_SAMPLE_PZ = 7 };   // initial-state sampling (lim_sample.cu)
 enum { MED_RT = 0, MED_BJORKEN = 1, MED_GRID = 2 };
+// The adjoint's tape: float4 rows per particle-step, row k of step s at
+// ((s - tape_first) * rows + k) * n + i.  Bjorken: (x0, x1, p0, p1), (p2, xi0, xi1, xi2).
+// 2+1D grid: the pre-step momentum and the medium the step saw, with its gradient, so
+// the reverse sweep needs no grid lookups:
+//   (p0, p1, p2, T), (xi0, xi1, xi2, v^x), (v^y, dT/dx, dT/dy, dv^x/dx), (dv^x/dy, dv^y/dx, dv^y/dy, 0)
+// (T before the medium scale, v the grid's flow velocity).
+__host__ __device__ constexpr int tape_rows(int med) { return med == MED_GRID ? 4 : 2; }
+constexpr int kTapeRowsMax = 4;
 enum { COLL_LANGEVIN = 0, COLL_RTA = 1, COLL_LANGEVIN_RTA = 2, COLL_FLUID = 3 };
 
 template <typename R> struct V2T;

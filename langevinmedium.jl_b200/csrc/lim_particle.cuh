@@ -68,7 +68,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && flag != 0.0) break;
         const StepRec<R> sr = tab[s];
-        if (REC == 2) {                   // the adjoint's tape: the pre-step state (the normals follow)
+        if (REC == 2 && MED != MED_GRID) {   // the adjoint's tape: the pre-step state (the normals follow)
             float4* t = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 2 * kp.n + i;
             *t = make_float4((float)x[0], (float)x[1], (float)p[0], (float)p[1]);
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];

@@ -140,8 +140,15 @@ __device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, in
     wy = fy - R(iy);
 }
 
-template <typename R>
-__device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R xq, R yq, R& T, R& ux, R& uy)
+// The grid medium at the particle with its gradient in (x, y) (zero along an axis where
+// the query is clamped to the grid), for the adjoint's tape.
+struct MedGrad {
+    float T, vx, vy, dT[2], dvx[2], dvy[2];
+};
+
+template <typename R, bool GRAD = false>
+__device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R xq, R yq, R& T, R& ux, R& uy,
+                                            MedGrad* mg = nullptr)
 {
     int ix, iy;
     R Wx, Wy;
@@ -161,6 +168,27 @@ __device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRe
     T = T0 * (R(1) - Wt) + T1 * Wt;
     ux = U0 * (R(1) - Wt) + U1 * Wt;
     uy = V0 * (R(1) - Wt) + V1 * Wt;
+    if constexpr (GRAD) {
+        const float wx = (float)Wx, wy = (float)Wy, wt = (float)Wt;
+        const float kx = (xq > (R)md.gx0_d && xq < (R)md.gxl_d) ? md.ginvdx : 0.0f;
+        const float ky = (yq > (R)md.gy0_d && yq < (R)md.gyl_d) ? md.ginvdy : 0.0f;
+        // d/dx: x-differences bilinear in (y, t); d/dy: y-differences bilinear in (x, t)
+        auto grad = [&](float A00, float A10, float A01, float A11, float B00, float B10, float B01, float B11,
+                        float (&g)[2]) {
+            const float xa = (A10 - A00) + wy * ((A11 - A01) - (A10 - A00));
+            const float xb = (B10 - B00) + wy * ((B11 - B01) - (B10 - B00));
+            const float ya = (A01 - A00) + wx * ((A11 - A10) - (A01 - A00));
+            const float yb = (B01 - B00) + wx * ((B11 - B10) - (B01 - B00));
+            g[0] = (xa + wt * (xb - xa)) * kx;
+            g[1] = (ya + wt * (yb - ya)) * ky;
+        };
+        grad(a00.x, a10.x, a01.x, a11.x, b00.x, b10.x, b01.x, b11.x, mg->dT);
+        grad(a00.y, a10.y, a01.y, a11.y, b00.y, b10.y, b01.y, b11.y, mg->dvx);
+        grad(a00.z, a10.z, a01.z, a11.z, b00.z, b10.z, b01.z, b11.z, mg->dvy);
+        mg->T = (float)T;
+        mg->vx = (float)ux;
+        mg->vy = (float)uy;
+    }
 }
 
 // Flow seen by one particle this step: boost direction (nx, ny), signed speed v,
@@ -171,8 +199,9 @@ struct Local {
     bool boost;   // false: r < eps (kernels_cpu.jl:75-77), or FP32 with zero flow
 };
 
-template <typename R, int MED, int DIMS>
-__device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3])
+template <typename R, int MED, int DIMS, bool GRAD = false>
+__device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
+                                                 MedGrad* mg = nullptr)
 {
     constexpr bool fp32 = sizeof(R) == 4;
     Local<R> L;
@@ -180,7 +209,7 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     if (MED == MED_GRID) {
         // the grid holds the flow velocity (v^x, v^y), as the reference's (r, t) tables do
         R ux, uy;
-        grid_lookup(kp.med, sr, x[0], x[1], L.T, ux, uy);
+        grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg);
         R u = sqrt(ux * ux + uy * uy);
         L.boost = !(u < R(kEps));
         L.v = u;
@@ -575,7 +604,18 @@ template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
 {
-    const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x);
+    // the grid medium's tape rows 0, 2, 3 (pre-step momentum, medium and gradient); row 1
+    // (the normals and v^x) follows the kick
+    constexpr bool kTapeGrid = REC == 2 && MED == MED_GRID;
+    MedGrad mg;
+    float4* trow = nullptr;
+    if constexpr (kTapeGrid) trow = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 4 * kp.n + i;
+    const Local<R> L = local_medium<R, MED, DIMS, kTapeGrid>(kp, sr, x, &mg);
+    if constexpr (kTapeGrid) {
+        trow[0] = make_float4((float)p[0], (float)p[1], (float)p[2], mg.T);
+        trow[2 * kp.n] = make_float4(mg.vy, mg.dT[0], mg.dT[1], mg.dvx[0]);
+        trow[3 * kp.n] = make_float4(mg.dvx[1], mg.dvy[0], mg.dvy[1], 0.0f);
+    }
     if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, false);
     if (PDIM == 3 && kp.redshift) p[2] *= sr.zf;
     if (kp.collision == COLL_FLUID) {
@@ -584,6 +624,9 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
         const R T = jmax0(L.T);
         const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_MOM);
         const bool kick = kp.collision != COLL_RTA;
+        if constexpr (kTapeGrid) {
+            if (!kick) trow[kp.n] = make_float4(0.0f, 0.0f, 0.0f, mg.vx);
+        }
         const bool rta = kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA;
         // one T-grid lookup for both splines when they share the grid
         const SplIdx<R> sd = spline_index(T, kp.drag_Tmin, kp.drag_invdT, kp.n_drag);
@@ -598,8 +641,12 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
                 xi[2] = R(0);
                 wc = u.z;
             }
+            if constexpr (kTapeGrid) {
+                trow[kp.n] = make_float4((float)xi[0], (float)xi[1], (float)xi[2], mg.vx);
+            } else {
 #pragma unroll
-            for (int d = 0; d < PDIM; ++d) rec_slot<REC>(kp, s, i, d, xi[d]);
+                for (int d = 0; d < PDIM; ++d) rec_slot<REC>(kp, s, i, d, xi[d]);
+            }
             const R tau = kp.DsT <= R(0) ? R(0) : spline_at(kp.drag, sd);
             langevin_kick<R, DIMS, PDIM>(kp, T, tau, p, xi);
         }

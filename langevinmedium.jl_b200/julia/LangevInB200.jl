@@ -86,6 +86,15 @@ function download_state!(c::Ctx, x::Matrix{Float64}, p::Matrix{Float64})
     return x, p
 end
 
+# sample_particles_from_FONLL (utils.jl:33-172) on the device; f is the (Np, Nr) density.
+function sample_fonll(c::Ctx, r_grid, p_grid, f, N::Integer; cartesian::Bool, antithetic::Bool, thermal_pz::Bool)
+    fm = Matrix{Float64}(size(f) == (length(p_grid), length(r_grid)) ? f : permutedims(f))
+    check(c.ptr, ccall((:lim_sample_fonll, libpath[]), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Cint, Cint, Cint),
+        c.ptr, Vector{Float64}(r_grid), length(r_grid), Vector{Float64}(p_grid), length(p_grid), fm, N,
+        cartesian, antithetic, thermal_pz))
+end
+
 initial_lab_boost(c::Ctx) = check(c.ptr, ccall((:lim_initial_lab_boost, libpath[]), Cint, (Ptr{Cvoid},), c.ptr))
 
 run!(c::Ctx, first_step, nsteps, save_every, hx, hp) =
@@ -126,18 +135,25 @@ function LM.Simulate.simulate_ensemble_bulk(
         save_every = max(steps, 1)
     end
     xgrid, tgrid = SpaceTimeGrid
-    (x_init === nothing || p_init === nothing) &&
-        error("B200Backend takes the initial state from x_init/p_init (sample it with LangevInMedium.Utils)")
-    positions = Matrix{Float64}(x_init); momenta = Matrix{Float64}(p_init)
-    radial_mode = dimensions == 1
     pdim = momentum_dimensions <= 0 ? dimensions : momentum_dimensions
-    LM.Utils.check_momentum_dims(dimensions, pdim, radial_mode, bjorken_redshift, initial_time)
-    if size(momenta, 1) < pdim
-        momenta = LM.Utils.append_thermal_pz(momenta, positions, m,
-            r -> LM.KernelsCPU.interpolate_2d_cpu(xgrid, tgrid, TemperatureEvolutionn, r, initial_time))
+    device_sampling = x_init === nothing || p_init === nothing
+    if device_sampling
+        # the FONLL sampler on the device (dimensions 2); other dimensions bring x_init/p_init
+        dimensions == 2 ||
+            error("B200Backend samples the FONLL initial state on the device for dimensions=2; pass x_init/p_init")
+        LM.Utils.check_momentum_dims(dimensions, pdim, false, bjorken_redshift, initial_time)
+        N = N_particles
+    else
+        positions = Matrix{Float64}(x_init); momenta = Matrix{Float64}(p_init)
+        radial_mode = dimensions == 1
+        LM.Utils.check_momentum_dims(dimensions, pdim, radial_mode, bjorken_redshift, initial_time)
+        if size(momenta, 1) < pdim
+            momenta = LM.Utils.append_thermal_pz(momenta, positions, m,
+                r -> LM.KernelsCPU.interpolate_2d_cpu(xgrid, tgrid, TemperatureEvolutionn, r, initial_time))
+        end
+        size(momenta, 1) == pdim || error("momentum rows $(size(momenta, 1)) ≠ momentum_dimensions $pdim")
+        N = size(positions, 2)
     end
-    size(momenta, 1) == pdim || error("momentum rows $(size(momenta, 1)) ≠ momentum_dimensions $pdim")
-    N = size(positions, 2)
 
     coll = (!momentum_langevin || DsT == 0.0) ? :fluid : collision_mode
     c = create(device)
@@ -165,7 +181,13 @@ function LM.Simulate.simulate_ensemble_bulk(
             set_invcdf(c, inv, nU, nT, Tm, Ti)
         end
     end
-    upload_state(c, positions, momenta)
+    if device_sampling
+        sample_fonll(c, r_grid_Langevin, p_grid_Langevin, heavy_quark_density, N;
+            cartesian = cartesian_spatial_sampling === nothing ? true : cartesian_spatial_sampling,
+            antithetic = antithetic_momenta, thermal_pz = pdim == 3)
+    else
+        upload_state(c, positions, momenta)
+    end
     initial_lab_boost(c)
     if freezeout_capture
         run!(c, 1, steps, 0, C_NULL, C_NULL)

@@ -59,7 +59,11 @@ def test_sample_matches_oracle(lmb, orc, prec, cart, anti, n, medium):
     assert failed == 0
     assert xd.shape == (2, n) and pd.shape == (3, n)
     assert np.max(np.abs(xd - xo)) <= 1e-12 * max(1.0, np.max(np.abs(xo)))
-    assert np.max(np.abs(pd - po)) <= 1e-12 * max(1.0, np.max(np.abs(po)))
+    assert np.max(np.abs(pd[:2] - po[:2])) <= 1e-12 * max(1.0, np.max(np.abs(po)))
+    # p_z: the FP32 state precision reads the medium from its FP32 tables, so the local
+    # temperature (and with it p_z) carries FP32 rounding there
+    tol_pz = 1e-12 if prec == "fp64" else 1e-6
+    assert np.max(np.abs(pd[2] - po[2])) <= tol_pz * max(1.0, np.max(np.abs(po[2])))
     assert np.any(po[2] != 0.0)
 
 
