@@ -287,6 +287,19 @@ int lim_adjoint_stats(lim_ctx* ctx, double* forward_ms, double* reverse_ms);
 int lim_sample_fonll(lim_ctx* ctx, const double* r_grid, int64_t nr, const double* p_grid, int64_t np,
                      const double* f, int64_t n, int cartesian, int antithetic, int thermal_pz);
 
+/* Samples n heavy quarks in Milne coordinates on the device into the state, replacing
+ * sample_initial_particles_milne! (utils.jl:350-400): nbins radial bins over
+ * [x_lo, x_hi] with the profiles T, u^r, mu evaluated at the bin centers
+ * (T_c, ur_c, mu_c: the host evaluates the reference's profile functions there), the
+ * binned Boltzmann density T^(3/2)/gamma exp((mu - m gamma)/T) sampled by rejection
+ * against the first bin center >= r, and p^r = sqrt(m T(r)) z with T(r) linear on the
+ * table (r_T, T_r) of nT ascending nodes.  State: (t0, r), (sqrt(m^2 + p_r^2), |p_r|).
+ * Draws: trial t from (seed, particle_offset + i, t, SAMPLE_XY), z from
+ * (seed, particle_offset + i, 0, SAMPLE_P).  Needs Milne coordinates (dimensions 2,
+ * pdim 2).  LIM_ERR_STATE when a particle found no accepted trial in 100000. */
+int lim_sample_milne(lim_ctx* ctx, double x_lo, double x_hi, int64_t nbins, const double* T_c, const double* ur_c,
+                     const double* mu_c, const double* r_T, const double* T_r, int64_t nT, int64_t n);
+
 /* ---- batches ------------------------------------------------------------------
  * Many independent ensembles — each a configured context with its own particle
  * count, step range, mass, transport tables and medium — advanced together: every

@@ -96,6 +96,8 @@ _SIGS = {
     "lim_copy_rta_decisions": ([C.c_void_p, C.c_void_p], C.c_int),
     "lim_adjoint": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
     "lim_adjoint_stats": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_sample_milne": ([C.c_void_p, C.c_double, C.c_double, C.c_int64, _DP, _DP, _DP, _DP, _DP, C.c_int64,
+                          C.c_int64], C.c_int),
     "lim_sample_fonll": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, _DP, C.c_int64, C.c_int, C.c_int, C.c_int],
                          C.c_int),
     "lim_batch_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
@@ -275,6 +277,20 @@ class Engine:
         fb = np.ascontiguousarray(fm.T).reshape(-1)
         self._check(self.lib.lim_sample_fonll(self.ctx, _dptr(rg), rg.size, _dptr(pg), pg.size, _dptr(fb), int(n),
                                               int(bool(cartesian)), int(bool(antithetic)), int(bool(thermal_pz))))
+        self.n = int(n)
+
+    def sample_milne(self, x_lo: float, x_hi: float, T_c, ur_c, mu_c, r_T, T_r, n: int):
+        """Sample n Milne (tau, r) particles on the device (lim_sample_milne): profiles
+        at the nbins bin centers of [x_lo, x_hi], T(r) on the table (r_T, T_r)."""
+        Tc = np.ascontiguousarray(T_c, dtype=np.float64)
+        uc = np.ascontiguousarray(ur_c, dtype=np.float64)
+        mc = np.ascontiguousarray(mu_c, dtype=np.float64)
+        rT = np.ascontiguousarray(r_T, dtype=np.float64)
+        TT = np.ascontiguousarray(T_r, dtype=np.float64)
+        if not (Tc.size == uc.size == mc.size) or rT.size != TT.size:
+            raise ValueError("the bin profiles and the T(r) table must have matching lengths")
+        self._check(self.lib.lim_sample_milne(self.ctx, float(x_lo), float(x_hi), Tc.size, _dptr(Tc), _dptr(uc),
+                                              _dptr(mc), _dptr(rT), _dptr(TT), rT.size, int(n)))
         self.n = int(n)
 
     def download_state(self):

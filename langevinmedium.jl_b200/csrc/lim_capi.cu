@@ -516,8 +516,10 @@ template int ctx_build_kparams<float>(lim_ctx*, KParams<float>&);
 
 namespace {
 
-template <typename R>
-int sample_impl(lim_ctx* c, const SampleTables& st_host, int64_t n)
+// Allocates the state for n particles and fills it with launch(kp) (a sampling kernel
+// that counts particles without an accepted trial in *failed).
+template <typename R, typename F>
+int sample_state(lim_ctx* c, int64_t n, unsigned long long* failed_dev, int max_trials, const char* who, F&& launch)
 {
     int rc;
     if ((rc = alloc_state<R>(c, n))) return rc;
@@ -530,17 +532,31 @@ int sample_impl(lim_ctx* c, const SampleTables& st_host, int64_t n)
     c->have_state = true;                 // the kernel parameters need the state buffers
     KParams<R> kp;
     if ((rc = build_kparams<R>(c, kp))) { c->have_state = false; return rc; }
-    LIM_CUDA(c, cudaMemsetAsync(st_host.failed, 0, sizeof(unsigned long long), c->stream));
-    LIM_CUDA(c, launch_sample_fonll<R>(kp, st_host, c->stream));
+    LIM_CUDA(c, cudaMemsetAsync(failed_dev, 0, sizeof(unsigned long long), c->stream));
+    LIM_CUDA(c, launch(kp));
     unsigned long long failed = 0;
-    LIM_CUDA(c, cudaMemcpyAsync(&failed, st_host.failed, sizeof failed, cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync(&failed, failed_dev, sizeof failed, cudaMemcpyDeviceToHost, c->stream));
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     if (failed) {
         c->have_state = false;
-        return fail(c, LIM_ERR_STATE, "lim_sample_fonll: %llu particles found no accepted trial in %d trials",
-                    failed, st_host.max_trials);
+        return fail(c, LIM_ERR_STATE, "%s: %llu particles found no accepted trial in %d trials", who, failed,
+                    max_trials);
     }
     return LIM_OK;
+}
+
+template <typename R>
+int sample_impl(lim_ctx* c, const SampleTables& st, int64_t n)
+{
+    return sample_state<R>(c, n, st.failed, st.max_trials, "lim_sample_fonll",
+                           [&](const KParams<R>& kp) { return launch_sample_fonll<R>(kp, st, c->stream); });
+}
+
+template <typename R>
+int sample_milne_impl(lim_ctx* c, const MilneTables& mt, int64_t n)
+{
+    return sample_state<R>(c, n, mt.failed, mt.max_trials, "lim_sample_milne",
+                           [&](const KParams<R>& kp) { return launch_sample_milne<R>(kp, mt, c->stream); });
 }
 
 }  // namespace
@@ -921,6 +937,66 @@ int lim_sample_fonll(lim_ctx* c, const double* r_grid, int64_t nr, const double*
     c->have_state = false;
     rc = c->P.precision == LIM_FP32 ? sample_impl<float>(c, st, n) : sample_impl<double>(c, st, n);
     LIM_CUDA(c, cudaStreamSynchronize(c->stream));    // the host tables are released on return
+    return rc;
+}
+
+int lim_sample_milne(lim_ctx* c, double x_lo, double x_hi, int64_t nbins, const double* T_c, const double* ur_c,
+                     const double* mu_c, const double* r_T, const double* T_r, int64_t nT, int64_t n)
+{
+    if (!c) return LIM_ERR_ARG;
+    ++c->gen;
+    int rc = state_rows_ok(c);
+    if (rc) return rc;
+    if (c->P.coords != LIM_COORDS_MILNE || c->P.dims != 2 || c->P.pdim != 2)
+        return fail(c, LIM_ERR_UNSUPPORTED, "Milne sampling requires dim = 2 (τ, r)");
+    if (n < 0 || n > (int64_t)UINT32_MAX) return fail(c, LIM_ERR_ARG, "lim_sample_milne: particle count out of range");
+    if (!T_c || !ur_c || !mu_c || !r_T || !T_r || nbins < 1 || nbins > INT32_MAX || nT < 2 || nT > INT32_MAX ||
+        !(x_hi > x_lo) || !std::isfinite(x_lo) || !std::isfinite(x_hi))
+        return fail(c, LIM_ERR_ARG, "lim_sample_milne: need x_lo < x_hi, nbins >= 1 profile values and a T(r) "
+                                    "table of at least 2 nodes");
+    if (!ascending(r_T, (size_t)nT)) return fail(c, LIM_ERR_ARG, "lim_sample_milne: r_T must be strictly ascending");
+    // utils.jl:356-373 in FP64: bin centers, n_boltz = T^(3/2)/gamma exp((mu - m gamma)/T), pdf = n/sum(n)/dx
+    const double m = c->P.m;
+    const double dx = (x_hi - x_lo) / (double)nbins;
+    std::vector<double> centers((size_t)nbins), nb((size_t)nbins), ratio((size_t)nbins);
+    double sum = 0.0;
+    for (int64_t k = 0; k < nbins; ++k) {
+        const double e0 = x_lo + dx * (double)k, e1 = x_lo + dx * (double)(k + 1);
+        centers[k] = (e0 + e1) / 2.0;
+        const double g = std::sqrt(1.0 + ur_c[k] * ur_c[k]);
+        nb[k] = std::pow(T_c[k], 1.5) / g * std::exp((mu_c[k] - m * g) / T_c[k]);
+        sum += nb[k];
+    }
+    double pmax = 0.0;
+    for (int64_t k = 0; k < nbins; ++k) { ratio[k] = nb[k] / sum / dx; pmax = std::max(pmax, ratio[k]); }
+    if (!(pmax > 0.0) || !std::isfinite(pmax))
+        return fail(c, LIM_ERR_ARG, "lim_sample_milne: the binned density has no positive finite maximum");
+    for (int64_t k = 0; k < nbins; ++k) ratio[k] /= pmax;
+    const size_t doubles = (size_t)(3 * nbins + 2 * nT);
+    cudaSetDevice(c->device);
+    if ((rc = dev_alloc(c, c->d_sample, doubles * sizeof(double) + 64))) return rc;
+    double* d = (double*)c->d_sample.p;
+    MilneTables mt;
+    std::memset(&mt, 0, sizeof mt);
+    mt.centers = d;
+    mt.ratio = d + nbins;
+    mt.rT = d + 2 * nbins;
+    mt.TT = d + 2 * nbins + nT;
+    mt.failed = (unsigned long long*)(((uintptr_t)(d + 2 * nbins + 2 * nT) + 15) & ~(uintptr_t)15);
+    LIM_CUDA(c, cudaMemcpyAsync((void*)mt.centers, centers.data(), nbins * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync((void*)mt.ratio, ratio.data(), nbins * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync((void*)mt.rT, r_T, nT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync((void*)mt.TT, T_r, nT * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    mt.nbins = (int)nbins;
+    mt.nT = (int)nT;
+    mt.lo = x_lo;
+    mt.hi = x_hi;
+    mt.max_trials = 100000;
+    c->dims = 2;
+    c->pdim = 2;
+    c->have_state = false;
+    rc = c->P.precision == LIM_FP32 ? sample_milne_impl<float>(c, mt, n) : sample_milne_impl<double>(c, mt, n);
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
     return rc;
 }
 

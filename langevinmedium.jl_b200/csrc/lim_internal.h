@@ -97,6 +97,18 @@ struct SampleTables {
 template <typename R>
 cudaError_t launch_sample_fonll(const KParams<R>& kp, const SampleTables& st, cudaStream_t s);
 
+// Milne (tau, r) sampling tables: the radial acceptance ratio pdf/max_pdf on nbins bin
+// centers and the temperature profile on an ascending r table (linear, clamped).
+struct MilneTables {
+    const double* centers; const double* ratio; int nbins;
+    const double* rT; const double* TT; int nT;
+    double lo, hi;
+    int max_trials;
+    unsigned long long* failed;
+};
+template <typename R>
+cudaError_t launch_sample_milne(const KParams<R>& kp, const MilneTables& mt, cudaStream_t s);
+
 cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStream_t st);
 
 // FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.

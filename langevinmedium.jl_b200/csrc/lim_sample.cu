@@ -158,6 +158,66 @@ k_sample_fonll(const KParams<R> kp, const SampleTables st)
     if (kp.pdim == 3) kp.p[2][i] = pz;
 }
 
+// sample_initial_particles_milne! (utils.jl:350-400): r by rejection against the binned
+// Boltzmann density (trial t: block (pid, t, SAMPLE_XY), r = lo + (hi - lo) u0 accepted if
+// u1 < pdf/max_pdf of the first bin center >= r), then p^r = sigma z with
+// sigma = sqrt(m T(r)) and z from block (pid, 0, SAMPLE_P); the state is (tau0, r),
+// (sqrt(m^2 + p_r^2), |p_r|).
+template <typename R>
+__global__ void __launch_bounds__(128)
+k_sample_milne(const KParams<R> kp, const MilneTables mt)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kp.n) return;
+    const NoiseKey nk{ kp.rk, (uint32_t)(kp.pid_offset + i) };
+    double r = 0.0;
+    bool ok = false;
+    for (int t = 0; t < mt.max_trials; ++t) {
+        const uint4 w = philox_words(nk.rk, nk.pid, (uint32_t)t, TAG_SAMPLE_XY);
+        const double rt = mt.lo + (mt.hi - mt.lo) * u_exact(w.x);
+        int lo = -1, hi = mt.nbins;                      // searchsortedfirst(centers, rt)
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (mt.centers[mid] >= rt) hi = mid; else lo = mid;
+        }
+        const double acc = hi < mt.nbins ? mt.ratio[hi] : 0.0;
+        if (u_exact(w.y) < acc) { r = rt; ok = true; break; }
+    }
+    if (!ok) atomicAdd(mt.failed, 1ull);
+    double T;
+    {
+        const double rq = fmin(fmax(r, mt.rT[0]), mt.rT[mt.nT - 1]);
+        const int k = cell_of(mt.rT, mt.nT, rq);
+        const double w = (rq - mt.rT[k]) / (mt.rT[k + 1] - mt.rT[k]);
+        T = mt.TT[k] + w * (mt.TT[k + 1] - mt.TT[k]);
+    }
+    const double sigma = sqrt((double)kp.m * T);
+    const uint4 v = philox_words(nk.rk, nk.pid, 0u, TAG_SAMPLE_P);
+    double z0, z1;
+    box_muller(v.x, v.y, z0, z1);
+    const double pr = sigma * z0;
+    const double tau0 = (double)kp.t0;
+    kp.x[0][i] = (R)tau0;
+    kp.x[1][i] = (R)r;
+    if (sizeof(R) == 4) {
+        kp.xlo[0][i] = (float)(tau0 - (double)(R)tau0);
+        kp.xlo[1][i] = (float)(r - (double)(R)r);
+    }
+    kp.p[0][i] = sqrt((double)kp.m * (double)kp.m + pr * pr);
+    kp.p[1][i] = fabs(pr);
+}
+
+template <typename R>
+cudaError_t launch_sample_milne(const KParams<R>& kp, const MilneTables& mt, cudaStream_t s)
+{
+    if (kp.n == 0) return cudaSuccess;
+    k_sample_milne<R><<<(unsigned)((kp.n + 127) / 128), 128, 0, s>>>(kp, mt);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_sample_milne<double>(const KParams<double>&, const MilneTables&, cudaStream_t);
+template cudaError_t launch_sample_milne<float>(const KParams<float>&, const MilneTables&, cudaStream_t);
+
 template <typename R>
 cudaError_t launch_sample_fonll(const KParams<R>& kp, const SampleTables& st, cudaStream_t s)
 {

@@ -39,6 +39,7 @@ struct LimParams
     block_size::Int64
 end
 
+const LIM_ERR_NONFINITE = Cint(-4)      # include/langevin_b200.h
 const LIM_COLL = Dict(:langevin => 0, :rta => 1, :langevin_rta => 2, :fluid => 3)
 
 mutable struct Ctx
@@ -201,6 +202,62 @@ function LM.Simulate.simulate_ensemble_bulk(
     run!(c, 1, steps, save_every, hx, hp)
     time_points = range(initial_time, final_time, length = num_saves + 1)
     return time_points, [hp[:, :, i] for i in 1:num_saves+1], [hx[:, :, i] for i in 1:num_saves+1]
+end
+
+# ---- simulate_ensemble_bulk(::B200_GCBackend, ...) — mirrors simulate.jl:117-141 ----------------
+# sample_initial_particles_milne! (utils.jl:350-400) runs on the device: the profiles are
+# evaluated at the 200 bin centers of (0, maximum(xgrid)), and T(r) for the momentum
+# width on a 1601-node table.
+function sample_milne(c::Ctx, x_lo, x_hi, Tc, urc, muc, rT, TT, N::Integer)
+    check(c.ptr, ccall((:lim_sample_milne, libpath[]), Cint,
+        (Ptr{Cvoid}, Float64, Float64, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Int64, Int64),
+        c.ptr, x_lo, x_hi, length(Tc), Tc, urc, muc, rT, TT, length(rT), N))
+end
+
+function LM.Simulate.simulate_ensemble_bulk(
+    backend::B200_GCBackend, T_profile_MIS, ur_profile_MIS, mu_profile_MIS,
+    TemperatureEvolutionn, VelocityEvolutionn, SpaceTimeGrid;
+    N_particles::Int = 10_000, Δt::Float64 = 0.001, initial_time::Float64 = 0.0, final_time::Float64 = 1.0,
+    save_interval::Float64 = 0.1, m::Float64 = 1.0, DsT::Float64 = 0.2, dimensions::Int = 2,
+    seed::Integer = 0x4C494D00, precision::Symbol = :fp64, device::Integer = 0)
+
+    @assert dimensions == 2 "Milne sampling requires dim = 2 (τ, r)"
+    steps = floor(Int, (final_time - initial_time) / Δt)
+    save_every = Int(save_interval / Δt)
+    num_saves = div(steps, save_every)
+    xgrid, tgrid = SpaceTimeGrid
+    c = create(device)
+    set_params(c, LimParams(Δt, initial_time, m, DsT, 0.0, 0.0, 5.0, 0.1, 2, 2, 1, LIM_COLL[:langevin],
+        1, 0, 0, 0, 0, 0, 1, precision == :fp32 ? 1 : 0, Int64(seed), 0, 0, 0))
+    set_medium_rt(c, xgrid, tgrid, TemperatureEvolutionn, VelocityEvolutionn, nothing)
+    if DsT > 0.0                                           # simulate_cpu_general_coords.jl:72-80
+        Tmin = max(float(minimum(TemperatureEvolutionn)), 0.0)
+        Tmax = max(float(maximum(TemperatureEvolutionn)), Tmin + eps(Float64))
+        t0_, invdT, dvals = LM.Transport.build_tau_drag_spline(m, DsT; Tmin = Tmin, Tmax = Tmax, nT = 1024)
+        set_spline(c, 0, t0_, invdT, dvals)
+    end
+    x_hi = float(maximum(xgrid))
+    edges = range(0.0, x_hi, length = 201)
+    centers = (edges[1:end-1] .+ edges[2:end]) ./ 2
+    rT = collect(range(0.0, x_hi, length = 1601))
+    sample_milne(c, 0.0, x_hi, Float64.(T_profile_MIS.(centers, initial_time)),
+        Float64.(ur_profile_MIS.(centers, initial_time)), Float64.(mu_profile_MIS.(centers, initial_time)),
+        rT, Float64.(T_profile_MIS.(rT, initial_time)), N_particles)
+    N = N_particles
+    hx = zeros(2, N, num_saves + 1)
+    hp = zeros(2, N, num_saves + 1)
+    x0 = zeros(2, N); p0 = zeros(2, N)
+    download_state!(c, x0, p0)
+    hx[:, :, 1] .= x0; hp[:, :, 1] .= p0
+    rc = ccall((:lim_run, libpath[]), Cint, (Ptr{Cvoid}, Int64, Int64, Int64, Int64, Ptr{Float64}, Ptr{Float64}),
+        c.ptr, 1, steps, save_every, 0, hx, hp)
+    rc == 0 || rc == LIM_ERR_NONFINITE || check(c.ptr, rc)   # the Milne CPU driver has no NaN/Inf check
+    time_points = range(initial_time, final_time, length = num_saves + 1)
+    # simulate_cpu_general_coords.jl:53-55, :120-124: |p^r| first, then |p| over (p^τ, p^r); the r row
+    momenta_history = [i == 1 ? abs.(hp[2, :, 1]) : vec(sqrt.(sum(hp[:, :, i] .^ 2, dims = 1))) for i in 1:num_saves+1]
+    position_history = [reshape(hx[2, :, i], 1, N) for i in 1:num_saves+1]
+    return time_points, momenta_history, position_history
 end
 
 end # module

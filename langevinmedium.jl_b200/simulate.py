@@ -208,6 +208,10 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
     return time_points, mom, pos
 
 
+MILNE_BINS = 200          # the reference's radial bins (simulate_cpu_general_coords.jl:41)
+MILNE_T_TABLE = 1601      # nodes of the T(r) table that sets the initial momentum width
+
+
 def _simulate_milne(T_profile_MIS, ur_profile_MIS, mu_profile_MIS, TemperatureEvolutionn, VelocityEvolutionn,
                     SpaceTimeGrid, *, N_particles: int = 10_000, Δt: float = 0.001, initial_time: float = 0.0,
                     final_time: float = 1.0, save_interval: float = 0.1, m: float = 1.0, DsT: float = 0.2,
@@ -225,11 +229,13 @@ def _simulate_milne(T_profile_MIS, ur_profile_MIS, mu_profile_MIS, TemperatureEv
     num_saves = steps // save_every
     xgrid, tgrid = SpaceTimeGrid
     Tfield = np.asarray(TemperatureEvolutionn, dtype=np.float64)
-    if x_init is None or p_init is None:
-        raise NotImplementedError("the B200 Milne backend takes the initial (τ, r), (p^τ, p^r) from x_init/p_init")
-    positions = np.array(x_init, dtype=np.float64, ndmin=2)
-    momenta = np.array(p_init, dtype=np.float64, ndmin=2)
-    N = positions.shape[1]
+    device_sampling = x_init is None or p_init is None
+    if device_sampling:
+        N = int(N_particles)
+    else:
+        positions = np.array(x_init, dtype=np.float64, ndmin=2)
+        momenta = np.array(p_init, dtype=np.float64, ndmin=2)
+        N = positions.shape[1]
     eng = _engine(device, stream)
     eng.set_params(dt=Δt, t0=initial_time, m=m, DsT=DsT, dims=2, pdim=2, coords=capi.LIM_COORDS_MILNE,
                    collision=capi.LIM_COLL_LANGEVIN, precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64,
@@ -240,7 +246,19 @@ def _simulate_milne(T_profile_MIS, ur_profile_MIS, mu_profile_MIS, TemperatureEv
         Tmin, Tmax = tr.spline_range(Tfield)
         t0_, inv_, vals = tr.build_tau_drag_spline(m, DsT, Tmin=Tmin, Tmax=Tmax, nT=1024)
         eng.set_spline(capi.LIM_SPLINE_DRAG, t0_, inv_, vals)
-    eng.upload_state(positions, momenta)
+    if device_sampling:
+        # sample_initial_particles_milne!(m, 2, N, τ0, profiles..., (0, maximum(xgrid)), 200)
+        # (simulate_cpu_general_coords.jl:40-41) on the device: the profiles are evaluated at
+        # the 200 bin centers, and T(r) for the momentum width on MILNE_T_TABLE nodes
+        x_hi = float(np.max(np.asarray(xgrid, dtype=np.float64)))
+        edges = np.linspace(0.0, x_hi, MILNE_BINS + 1)
+        centers = (edges[:-1] + edges[1:]) / 2
+        prof = lambda f, rs: np.array([float(f(r, initial_time)) for r in rs])
+        r_T = np.linspace(0.0, x_hi, MILNE_T_TABLE)
+        eng.sample_milne(0.0, x_hi, prof(T_profile_MIS, centers), prof(ur_profile_MIS, centers),
+                         prof(mu_profile_MIS, centers), r_T, prof(T_profile_MIS, r_T), N)
+    else:
+        eng.upload_state(positions, momenta)
     nslots = num_saves + 1
     hx = np.empty(nslots * N * 2)
     hp = np.empty(nslots * N * 2)

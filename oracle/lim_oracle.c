@@ -1048,3 +1048,58 @@ done:
     free(cdf_p); free(nsp); free(cdf_r); free(mass);
     return failed;
 }
+
+/* utils.jl:350-400 sample_initial_particles_milne!, with the particle's counter-based
+ * draws (trial t: block (pid, t, SAMPLE_XY); p_r: block (pid, 0, SAMPLE_P)) and T(r)
+ * linear on (r_T, T_r).  x (2, n) = (t0, r), p (2, n) = (p^tau, |p^r|).  Returns the
+ * number of particles without an accepted trial, or -1 for a density without a
+ * positive finite maximum. */
+int64_t orc_sample_milne(const orc_params* P, double x_lo, double x_hi, int64_t nbins, const double* T_c,
+                         const double* ur_c, const double* mu_c, const double* r_T, const double* T_r, int64_t nT,
+                         int64_t n, double* x, double* p)
+{
+    const double m = P->m, dx = (x_hi - x_lo) / (double)nbins;
+    double* centers = calloc((size_t)nbins, sizeof(double));
+    double* ratio = calloc((size_t)nbins, sizeof(double));
+    double sum = 0.0, pmax = 0.0;
+    int64_t failed = 0;
+    for (int64_t k = 0; k < nbins; ++k) {
+        double e0 = x_lo + dx * (double)k, e1 = x_lo + dx * (double)(k + 1);
+        centers[k] = (e0 + e1) / 2.0;
+        double g = sqrt(1.0 + ur_c[k] * ur_c[k]);
+        ratio[k] = pow(T_c[k], 1.5) / g * exp((mu_c[k] - m * g) / T_c[k]);
+        sum += ratio[k];
+    }
+    for (int64_t k = 0; k < nbins; ++k) { ratio[k] = ratio[k] / sum / dx; pmax = ratio[k] > pmax ? ratio[k] : pmax; }
+    if (!(pmax > 0.0) || !isfinite(pmax)) { failed = -1; goto done; }
+    for (int64_t k = 0; k < nbins; ++k) ratio[k] /= pmax;
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t pid = P->particle_offset + i;
+        double r = 0.0;
+        int ok = 0;
+        for (int t = 0; t < 100000 && !ok; ++t) {
+            uint32_t w[4];
+            words(P, pid, t, TAG_SAMPLE_XY, w);
+            double rt = x_lo + (x_hi - x_lo) * u01(w[0]);
+            int64_t idx = 0;                         /* searchsortedfirst(centers, rt) */
+            while (idx < nbins && centers[idx] < rt) ++idx;
+            double acc = idx < nbins ? ratio[idx] : 0.0;
+            if (u01(w[1]) < acc) { r = rt; ok = 1; }
+        }
+        if (!ok) ++failed;
+        double rq = jl_clamp(r, r_T[0], r_T[nT - 1]);
+        int64_t k = ss_last(r_T, nT, rq);
+        double wk = (rq - r_T[k]) / (r_T[k + 1] - r_T[k]);
+        double T = T_r[k] + wk * (T_r[k + 1] - T_r[k]);
+        uint32_t v[4];
+        double z0, z1;
+        words(P, pid, 0, TAG_SAMPLE_P, v);
+        box_muller(u01(v[0]), u01(v[1]), &z0, &z1);
+        double pr = sqrt(m * T) * z0;
+        x[2 * i] = P->t0; x[2 * i + 1] = r;
+        p[2 * i] = sqrt(m * m + pr * pr); p[2 * i + 1] = fabs(pr);
+    }
+done:
+    free(centers); free(ratio);
+    return failed;
+}

@@ -86,6 +86,9 @@ def lib() -> C.CDLL:
         L.orc_sample_fonll.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcMedium), _DP, C.c_int64, _DP, C.c_int64,
                                        _DP, C.c_int64, C.c_int, C.c_int, C.c_int, _DP, _DP]
         L.orc_sample_fonll.restype = C.c_int64
+        L.orc_sample_milne.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, _DP, _DP, _DP, _DP,
+                                       _DP, C.c_int64, C.c_int64, _DP, _DP]
+        L.orc_sample_milne.restype = C.c_int64
         L.orc_sample_pz.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, _DP]
         L.orc_sample_pz.restype = None
         assert L.orc_sizeof_params() == C.sizeof(OrcParams)
@@ -268,3 +271,13 @@ def sample_pz(P: OrcParams, mT, T, n):
     out = np.zeros(max(int(n), 1))
     lib().orc_sample_pz(C.byref(P), float(mT), float(T), int(n), _d(out))
     return out[:int(n)]
+
+
+def sample_milne(P: OrcParams, x_lo, x_hi, T_c, ur_c, mu_c, r_T, T_r, n):
+    """Restatement of the device Milne sampler.  Returns (x (2, n), p (2, n), failed)."""
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (T_c, ur_c, mu_c, r_T, T_r)]
+    xb = np.zeros(max(2 * n, 1))
+    pb = np.zeros(max(2 * n, 1))
+    failed = lib().orc_sample_milne(C.byref(P), float(x_lo), float(x_hi), a[0].size, _d(a[0]), _d(a[1]), _d(a[2]),
+                                    _d(a[3]), _d(a[4]), a[3].size, int(n), _d(xb), _d(pb))
+    return from_flat(xb[:2 * n], 2, n), from_flat(pb[:2 * n], 2, n), int(failed)

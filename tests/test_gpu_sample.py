@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from helpers import oracle_drive, parity
-from test_sample_oracle import fonll_like
+from test_sample_oracle import fonll_like, milne_profiles
 
 pytestmark = pytest.mark.gpu
 
@@ -117,3 +117,59 @@ def test_run_from_device_sample(lmb, orc, prec):
         assert (emax if prec == "fp64" else e99) <= tol, (k, emax, e99)
         emax, e99 = parity(pos[k], xh[k], 1.0)
         assert (emax if prec == "fp64" else e99) <= tol, (k, emax, e99)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [1, 777, 20_000])
+def test_milne_sample_matches_oracle(lmb, orc, prec, n):
+    c, Tc, urc, muc, Tf = milne_profiles()
+    rT = np.linspace(0.0, 10.0, 1601)
+    e = lmb.capi.Engine(0)
+    e.set_params(dims=2, pdim=2, coords=lmb.capi.LIM_COORDS_MILNE, t0=0.4, m=1.5, dt=0.01, seed=SEED,
+                 particle_offset=5, precision=lmb.capi.LIM_FP32 if prec == "fp32" else lmb.capi.LIM_FP64)
+    e.sample_milne(0.0, 10.0, Tc, urc, muc, rT, Tf(rT), n)
+    xd, pd = e.download_state()
+    P = orc.make_params(seed=SEED, dims=2, pdim=2, m=1.5, t0=0.4, particle_offset=5)
+    xo, po, failed = orc.sample_milne(P, 0.0, 10.0, Tc, urc, muc, rT, Tf(rT), n)
+    assert failed == 0
+    assert np.max(np.abs(xd - xo)) <= 1e-12 * 10
+    assert np.max(np.abs(pd - po)) <= 1e-12 * max(1.0, np.max(np.abs(po)))
+
+
+def test_milne_sample_errors(lmb):
+    c, Tc, urc, muc, Tf = milne_profiles(nbins=4)
+    rT = np.linspace(0.0, 10.0, 5)
+    e = lmb.capi.Engine(0)
+    e.set_params(dims=2, pdim=2, coords=lmb.capi.LIM_COORDS_MILNE, t0=0.4, m=1.5, dt=0.01)
+    with pytest.raises(RuntimeError, match="no positive finite maximum"):
+        e.sample_milne(0.0, 10.0, np.zeros(4), urc, muc, rT, Tf(rT), 8)
+    ec = _engine(lmb, "fp64", 2)
+    with pytest.raises(RuntimeError, match="requires dim = 2"):
+        ec.sample_milne(0.0, 10.0, Tc, urc, muc, rT, Tf(rT), 8)
+
+
+def test_milne_run_from_device_sample(lmb, orc):
+    """simulate_ensemble_bulk(B200_GCBackend()) without x_init samples on the device: the
+    first snapshot is the oracle's sample (|p^r| and r), and the run stays finite."""
+    c, Tc, urc, muc, Tf = milne_profiles()
+    xg = np.linspace(0.0, 10.0, 41)
+    tg = np.linspace(0.4, 2.4, 21)
+    T = (0.42 * np.exp(-xg[:, None] ** 2 / 30.0) + 0.05) * (0.4 / tg[None, :]) ** (1 / 3)
+    V = 0.05 * xg[:, None] * np.ones_like(tg)[None, :]
+    prof_T = lambda r, tau: 0.42 * np.exp(-r ** 2 / 30.0) + 0.05
+    prof_ur = lambda r, tau: 0.04 * r
+    prof_mu = lambda r, tau: 0.02 * np.sin(r)
+    N = 4000
+    t, mom, pos = lmb.simulate_ensemble_bulk(lmb.B200_GCBackend(), prof_T, prof_ur, prof_mu, T, V, (xg, tg),
+                                             N_particles=N, Δt=0.01, initial_time=0.4, final_time=0.9,
+                                             save_interval=0.25, m=1.5, DsT=0.3, seed=SEED)
+    P = orc.make_params(seed=SEED, dims=2, pdim=2, m=1.5, t0=0.4)
+    edges = np.linspace(0.0, 10.0, 201)
+    cen = (edges[:-1] + edges[1:]) / 2
+    rT = np.linspace(0.0, 10.0, 1601)
+    xo, po, failed = orc.sample_milne(P, 0.0, 10.0, prof_T(cen, 0.4), prof_ur(cen, 0.4), prof_mu(cen, 0.4), rT,
+                                      prof_T(rT, 0.4), N)
+    assert failed == 0
+    assert np.max(np.abs(pos[0][0] - xo[1])) <= 1e-12 * 10
+    assert np.max(np.abs(mom[0] - po[1])) <= 1e-12 * 10
+    assert len(mom) == 3 and np.all(np.isfinite(mom[-1])) and np.all(np.isfinite(pos[-1]))

@@ -1,4 +1,5 @@
-"""The oracle's initial-state sampler (the checker of lim_sample_fonll) against the
+"""The oracle's initial-state samplers (the checkers of lim_sample_fonll and
+lim_sample_milne) against the
 reference's own statements about it:
 
 * test_momentum_dims3.jl:98-117 (S): the conditional p_z draw has the thermal <p_z^2>
@@ -6,7 +7,10 @@ reference's own statements about it:
   antithetic pairs mirror p_z exactly;
 * utils.jl:33-172: the position density is n(r) (Cartesian mode) or the r marginal of
   r p f (polar mode), and |p| | r follows the row CDF built from p f(r, p) — checked by
-  Kolmogorov–Smirnov tests against those CDFs, restated here in numpy.
+  Kolmogorov–Smirnov tests against those CDFs, restated here in numpy;
+* utils.jl:350-400: the Milne sampler's r follows the binned Boltzmann density (the
+  first bin center >= r decides), p^r is half-normal with sigma = sqrt(m T(r)) and p^tau
+  is on shell.
 """
 import numpy as np
 import pytest
@@ -143,3 +147,41 @@ def test_zero_density(orc):
     P = orc.make_params(seed=15, dims=2, pdim=2)
     _, _, failed = orc.sample_fonll(P, None, r, p, np.zeros((5, 5)), 3, cartesian=False)
     assert failed == -1                                     # "Distribution normalization is zero."
+
+
+def milne_profiles(nbins=200, x_hi=10.0):
+    c = (np.arange(nbins) + 0.5) * x_hi / nbins
+    T = lambda r: 0.42 * np.exp(-np.asarray(r) ** 2 / 30.0) + 0.05
+    return c, T(c), 0.04 * c, 0.02 * np.sin(c), T
+
+
+def test_milne_sampler_follows_the_binned_density(orc):
+    """utils.jl:356-399: r by rejection against the binned n_boltz (the first bin center
+    >= r decides), p^r half-normal with sigma = sqrt(m T(r)), p^tau on shell."""
+    m, x_hi, n = 1.5, 10.0, 20_000
+    c, Tc, urc, muc, Tf = milne_profiles(x_hi=x_hi)
+    rT = np.linspace(0.0, x_hi, 1601)
+    P = orc.make_params(seed=21, dims=2, pdim=2, m=m, t0=0.4)
+    x, p, failed = orc.sample_milne(P, 0.0, x_hi, Tc, urc, muc, rT, Tf(rT), n)
+    assert failed == 0
+    assert np.all(x[0] == 0.4)
+    g = np.sqrt(1 + urc ** 2)
+    nb = Tc ** 1.5 / g * np.exp((muc - m * g) / Tc)
+    # density of r: nb[k] on (c[k-1], c[k]] (k = 0 from x_lo), 0 beyond the last center
+    edges = np.concatenate([[0.0], c])
+    mass = nb * np.diff(edges)
+    cdf_nodes = np.concatenate([[0.0], np.cumsum(mass)]) / mass.sum()
+    assert stats.kstest(x[1], lambda v: np.interp(v, edges, cdf_nodes)).pvalue > 1e-3
+    sig = np.sqrt(m * np.interp(x[1], rT, Tf(rT)))
+    u = 2 * stats.norm.cdf(p[1] / sig) - 1
+    assert stats.kstest(u, "uniform").pvalue > 1e-3
+    assert np.allclose(p[0], np.sqrt(m * m + p[1] ** 2), rtol=1e-15)
+    assert np.all(p[1] >= 0)
+
+
+def test_milne_sampler_degenerate_density(orc):
+    c, Tc, urc, muc, Tf = milne_profiles(nbins=4)
+    P = orc.make_params(seed=22, dims=2, pdim=2, m=1.5)
+    rT = np.linspace(0, 10, 5)
+    _, _, failed = orc.sample_milne(P, 0.0, 10.0, np.zeros(4), urc, muc, rT, Tf(rT), 3)
+    assert failed == -1
