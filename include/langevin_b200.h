@@ -205,6 +205,34 @@ int lim_run(lim_ctx* ctx, int64_t first_step, int64_t nsteps,
             int64_t save_every, int64_t first_slot,
             double* hist_x, double* hist_p);
 
+/* ---- snapshots reduced on the device ---------------------------------------------
+ * In place of the FP64 snapshot history (simulate_cpu.jl:319-322: pdim x N x nslots
+ * momenta and positions, 38 GB for 1e7 particles and 95 saves), each snapshot is
+ * reduced on the device to, per slot (stride = lim_reduce_stride(spec) doubles):
+ *   [0, LIM_OBS_NUM)            the observable sums of lim_observables
+ *   r_bins + 1                  counts of r = |x| (Milne: the r row) in uniform bins on
+ *                               [0, r_max), the last entry counting r >= r_max: the
+ *                               radial density n(r, t) (exported as n_rt, LangevInMedium.jl:44)
+ *   pt_bins + 1                 counts of p_T = |(p_x, p_y)| (Milne: |p^r|), same binning
+ *   pt_bins + 1                 sums of cos 2 phi_p per p_T bin (0 for Milne), each term
+ *                               rounded to 2^-32: the numerator of v2(p_T)
+ * Counts are exact; the cos 2 phi sums are exact sums of the rounded terms, so the
+ * result does not depend on the order of summation. */
+typedef struct lim_reduce_spec {
+    int64_t r_bins;         /* 1 .. 4096 */
+    double r_max;           /* fm */
+    int64_t pt_bins;        /* 1 .. 4096 */
+    double pt_max;          /* GeV */
+} lim_reduce_spec;
+int64_t lim_reduce_stride(const lim_reduce_spec* spec);
+/* Reduce the current state into out[lim_reduce_stride(spec)]. */
+int lim_reduce_state(lim_ctx* ctx, const lim_reduce_spec* spec, double* out);
+/* lim_run whose snapshots (steps s with s % save_every == 0, slot s / save_every -
+ * first_slot, slots outside [0, nslots) skipped) are reduced on the device instead of
+ * copied; out holds nslots x lim_reduce_stride(spec) doubles, written once at the end. */
+int lim_run_reduced(lim_ctx* ctx, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
+                    int64_t nslots, const lim_reduce_spec* spec, double* out);
+
 /* First step at which a particle became non-finite, or -1. */
 int lim_status(lim_ctx* ctx, int64_t* first_bad_step);
 

@@ -61,6 +61,23 @@ class LimBatchShape(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class LimReduceSpec(C.Structure):
+    _fields_ = [("r_bins", C.c_int64), ("r_max", C.c_double), ("pt_bins", C.c_int64), ("pt_max", C.c_double)]
+
+
+def reduce_spec(r_bins: int, r_max: float, pt_bins: int, pt_max: float) -> LimReduceSpec:
+    return LimReduceSpec(int(r_bins), float(r_max), int(pt_bins), float(pt_max))
+
+
+def split_reduced(out: np.ndarray, spec: LimReduceSpec) -> dict:
+    """(nslots, stride) doubles of lim_run_reduced / lim_reduce_state -> named arrays."""
+    nr, npt = int(spec.r_bins) + 1, int(spec.pt_bins) + 1
+    o = out.reshape(-1, LIM_OBS_NUM + nr + 2 * npt)
+    return dict(obs=o[:, :LIM_OBS_NUM].copy(), r_counts=o[:, LIM_OBS_NUM:LIM_OBS_NUM + nr].copy(),
+                pt_counts=o[:, LIM_OBS_NUM + nr:LIM_OBS_NUM + nr + npt].copy(),
+                pt_cos2=o[:, LIM_OBS_NUM + nr + npt:].copy())
+
+
 _SIGS = {
     "lim_abi_version": ([], C.c_int),
     "lim_create": ([C.c_int, C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
@@ -96,6 +113,10 @@ _SIGS = {
     "lim_copy_rta_decisions": ([C.c_void_p, C.c_void_p], C.c_int),
     "lim_adjoint": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
     "lim_adjoint_stats": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_reduce_stride": ([C.POINTER(LimReduceSpec)], C.c_int64),
+    "lim_reduce_state": ([C.c_void_p, C.POINTER(LimReduceSpec), _DP], C.c_int),
+    "lim_run_reduced": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.POINTER(LimReduceSpec),
+                         _DP], C.c_int),
     "lim_sample_milne": ([C.c_void_p, C.c_double, C.c_double, C.c_int64, _DP, _DP, _DP, _DP, _DP, C.c_int64,
                           C.c_int64], C.c_int),
     "lim_sample_fonll": ([C.c_void_p, _DP, C.c_int64, _DP, C.c_int64, _DP, C.c_int64, C.c_int, C.c_int, C.c_int],
@@ -316,6 +337,20 @@ class Engine:
             hist_x: np.ndarray | None = None, hist_p: np.ndarray | None = None):
         self._check(self.lib.lim_run(self.ctx, int(first_step), int(nsteps), int(save_every), int(first_slot),
                                      _dptr(hist_x), _dptr(hist_p)))
+
+    def reduce_state(self, spec: LimReduceSpec) -> dict:
+        """The current state reduced on the device (lim_reduce_state): one slot."""
+        out = np.zeros(max(int(self.lib.lim_reduce_stride(C.byref(spec))), 1))   # an invalid spec fails below
+        self._check(self.lib.lim_reduce_state(self.ctx, C.byref(spec), _dptr(out)))
+        return {k: v[0] for k, v in split_reduced(out, spec).items()}
+
+    def run_reduced(self, first_step: int, nsteps: int, save_every: int, first_slot: int, nslots: int,
+                    spec: LimReduceSpec) -> dict:
+        """run() with every snapshot reduced on the device (lim_run_reduced)."""
+        out = np.zeros(max(nslots * int(self.lib.lim_reduce_stride(C.byref(spec))), 1))
+        self._check(self.lib.lim_run_reduced(self.ctx, int(first_step), int(nsteps), int(save_every),
+                                             int(first_slot), int(nslots), C.byref(spec), _dptr(out)))
+        return split_reduced(out, spec)
 
     def status(self) -> int:
         v = C.c_int64(-1)

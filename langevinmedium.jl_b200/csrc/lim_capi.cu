@@ -271,15 +271,33 @@ int block_of(const lim_ctx* c)
 
 constexpr int64_t kLiveSteps = 32;   // steps between compactions of the live list
 
+// A snapshot reduced on the device into slot `slot` of the reduction buffers (observable
+// sums and histograms; see lim_run_reduced).
+struct SnapshotReduce {
+    ReduceSpec rs;
+    int64_t nslots;
+};
+
+template <typename R>
+int reduce_snapshot(lim_ctx* c, const KParams<R>& kp, const SnapshotReduce& red, int64_t slot)
+{
+    double* obs = (double*)c->d_red_obs.p + slot * kObsNum;
+    unsigned long long* hist = (unsigned long long*)c->d_red_hist.p + slot * reduce_hist_len(red.rs);
+    LIM_CUDA(c, launch_reduce_hist<R>(kp, c->P.coords == LIM_COORDS_MILNE, red.rs, hist, c->P.obs_pt_cut,
+                                      c->P.obs_pt_width > 0 ? c->P.obs_pt_width : 1e-3, (double*)c->d_partials.p, obs,
+                                      c->stream));
+    return LIM_OK;
+}
+
 template <typename R>
 int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
-             double* hist_x, double* hist_p)
+             double* hist_x, double* hist_p, const SnapshotReduce* red = nullptr)
 {
     KParams<R> kp;
     int rc = build_kparams<R>(c, kp);
     if (rc) return rc;
     const int block = block_of(c);
-    const bool saving = save_every > 0 && (hist_x || hist_p);
+    const bool saving = save_every > 0 && (hist_x || hist_p || red);
     const int64_t end = first_step + nsteps;
     const int64_t chunk_max = saving ? std::min<int64_t>(nsteps, save_every) : nsteps;
     if ((rc = dev_alloc(c, c->d_steps, (size_t)std::max<int64_t>(chunk_max, 1) * step_record_bytes<R>()))) return rc;
@@ -329,7 +347,13 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
             kp.live_n = nullptr;
         }
         const int64_t last = chunk_end - 1;
-        if (saving && last % save_every == 0 && last >= 0) {
+        if (red && saving && last % save_every == 0 && last >= 0) {
+            const int64_t slot = last / save_every - first_slot;
+            if (slot >= 0 && slot < red->nslots) {
+                if ((rc = reduce_snapshot<R>(c, kp, *red, slot))) return rc;
+                launches += 2;
+            }
+        } else if (saving && last % save_every == 0 && last >= 0) {
             const int64_t slot = last / save_every - first_slot;
             if (slot >= 0) {
                 R* xs[3] = { kp.x[0], kp.x[1], kp.x[2] };
@@ -605,7 +629,8 @@ int lim_destroy(lim_ctx* c)
                       &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
-                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample };
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
+                      &c->d_red_obs, &c->d_red_hist };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -635,7 +660,8 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
                             &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
-                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample };
+                      &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
+                      &c->d_red_obs, &c->d_red_hist };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -1107,6 +1133,104 @@ int lim_run(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, 
     cudaSetDevice(c->device);
     return c->state_prec == LIM_FP32 ? run_impl<float>(c, first_step, nsteps, save_every, first_slot, hist_x, hist_p)
                                      : run_impl<double>(c, first_step, nsteps, save_every, first_slot, hist_x, hist_p);
+}
+
+}  // extern "C"
+
+namespace {
+
+int reduce_setup(lim_ctx* c, const lim_reduce_spec* spec, int64_t nslots, SnapshotReduce& red)
+{
+    if (!spec || spec->r_bins < 1 || spec->r_bins > kReduceBinsMax || spec->pt_bins < 1 ||
+        spec->pt_bins > kReduceBinsMax || !(spec->r_max > 0.0) || !(spec->pt_max > 0.0) ||
+        !std::isfinite(spec->r_max) || !std::isfinite(spec->pt_max))
+        return fail(c, LIM_ERR_ARG, "lim_reduce_spec: need 1..%d bins and finite positive r_max, pt_max",
+                    kReduceBinsMax);
+    red.rs.r_bins = (int)spec->r_bins;
+    red.rs.pt_bins = (int)spec->pt_bins;
+    red.rs.r_scale = (double)spec->r_bins / spec->r_max;
+    red.rs.pt_scale = (double)spec->pt_bins / spec->pt_max;
+    red.nslots = nslots;
+    const int64_t nb = c->n == 0 ? 1 : (c->n + 255) / 256;
+    int rc;
+    if ((rc = dev_alloc(c, c->d_partials, (size_t)nb * kObsNum * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_red_obs, (size_t)nslots * kObsNum * sizeof(double)))) return rc;
+    if ((rc = dev_alloc(c, c->d_red_hist, (size_t)nslots * reduce_hist_len(red.rs) * sizeof(unsigned long long))))
+        return rc;
+    LIM_CUDA(c, cudaMemsetAsync(c->d_red_obs.p, 0, (size_t)nslots * kObsNum * sizeof(double), c->stream));
+    LIM_CUDA(c, cudaMemsetAsync(c->d_red_hist.p, 0, (size_t)nslots * reduce_hist_len(red.rs) * sizeof(unsigned long long),
+                                c->stream));
+    return LIM_OK;
+}
+
+// The device slots into out (host): per slot LIM_OBS_NUM sums, then the histograms as
+// doubles (counts exact; the cos 2 phi sums from their 2^-32 fixed point).
+int reduce_download(lim_ctx* c, const SnapshotReduce& red, double* out)
+{
+    const int64_t hl = reduce_hist_len(red.rs), stride = kObsNum + hl;
+    std::vector<double> obs((size_t)red.nslots * kObsNum);
+    std::vector<unsigned long long> hist((size_t)(red.nslots * hl));
+    LIM_CUDA(c, cudaMemcpyAsync(obs.data(), c->d_red_obs.p, obs.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    LIM_CUDA(c, cudaMemcpyAsync(hist.data(), c->d_red_hist.p, hist.size() * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int64_t ncount = red.rs.r_bins + 1 + red.rs.pt_bins + 1;
+    for (int64_t k = 0; k < red.nslots; ++k) {
+        double* o = out + k * stride;
+        for (int j = 0; j < kObsNum; ++j) o[j] = obs[(size_t)(k * kObsNum + j)];
+        const unsigned long long* h = hist.data() + k * hl;
+        for (int64_t j = 0; j < hl; ++j)
+            o[kObsNum + j] = j < ncount ? (double)h[j] : (double)(long long)h[j] * 0x1p-32;
+    }
+    return LIM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t lim_reduce_stride(const lim_reduce_spec* spec)
+{
+    if (!spec || spec->r_bins < 1 || spec->pt_bins < 1) return -1;
+    return LIM_OBS_NUM + spec->r_bins + 1 + 2 * (spec->pt_bins + 1);
+}
+
+int lim_reduce_state(lim_ctx* c, const lim_reduce_spec* spec, double* out)
+{
+    if (!c || !out) return LIM_ERR_ARG;
+    int rc = check_ready(c);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    SnapshotReduce red;
+    if ((rc = reduce_setup(c, spec, 1, red))) return rc;
+    if (c->state_prec == LIM_FP32) {
+        KParams<float> kp;
+        if ((rc = build_kparams<float>(c, kp)) || (rc = reduce_snapshot<float>(c, kp, red, 0))) return rc;
+    } else {
+        KParams<double> kp;
+        if ((rc = build_kparams<double>(c, kp)) || (rc = reduce_snapshot<double>(c, kp, red, 0))) return rc;
+    }
+    return reduce_download(c, red, out);
+}
+
+int lim_run_reduced(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
+                    int64_t nslots, const lim_reduce_spec* spec, double* out)
+{
+    if (!c || !out) return LIM_ERR_ARG;
+    int rc = check_ready(c);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(c, LIM_ERR_ARG, "lim_run_reduced: negative step count");
+    if (first_step < 0 || first_step + nsteps > (int64_t)UINT32_MAX)
+        return fail(c, LIM_ERR_ARG, "lim_run_reduced: steps must lie in [0, 2^32)");
+    if (save_every < 1 || nslots < 1) return fail(c, LIM_ERR_ARG, "lim_run_reduced: need save_every >= 1 and nslots >= 1");
+    cudaSetDevice(c->device);
+    SnapshotReduce red;
+    if ((rc = reduce_setup(c, spec, nslots, red))) return rc;
+    rc = c->state_prec == LIM_FP32 ? run_impl<float>(c, first_step, nsteps, save_every, first_slot, nullptr, nullptr, &red)
+                                   : run_impl<double>(c, first_step, nsteps, save_every, first_slot, nullptr, nullptr, &red);
+    if (rc) return rc;
+    return reduce_download(c, red, out);
 }
 
 int lim_status(lim_ctx* c, int64_t* first_bad_step)

@@ -55,6 +55,7 @@ struct lim_ctx {
     lim::DevBuf d_live[2], d_live_n;      // live lists of a stop-at-freeze-out run
     lim::DevBuf d_rta_bits;               // recorded / replayed RTA decisions
     lim::DevBuf d_sample;                 // sampling tables (lim_sample_fonll)
+    lim::DevBuf d_red_obs, d_red_hist;    // snapshot reductions (lim_run_reduced)
     int rta_mode = 0;
     int64_t rta_first = 0, rta_steps = 0;
     lim::DevBuf d_adj_ckpt, d_adj_tape, d_adj_table, d_adj_part, d_adj_out;   // lim_adjoint

@@ -97,6 +97,23 @@ struct SampleTables {
 template <typename R>
 cudaError_t launch_sample_fonll(const KParams<R>& kp, const SampleTables& st, cudaStream_t s);
 
+// Snapshot reduction (lim_reduce.cu): uniform bins on [0, r_max) and [0, pt_max), each
+// with one overflow entry; scale = bins / max.
+struct ReduceSpec {
+    int r_bins, pt_bins;
+    double r_scale, pt_scale;
+};
+constexpr int kReduceBinsMax = 4096;
+inline int64_t reduce_hist_len(const ReduceSpec& rs) { return (int64_t)rs.r_bins + 1 + 2 * ((int64_t)rs.pt_bins + 1); }
+// The histograms of the state and its observable sums (obs_out, kObsNum doubles);
+// partials holds reduce_grid(n) x kObsNum doubles.
+int reduce_grid(int64_t n);
+template <typename R>
+cudaError_t launch_reduce_hist(const KParams<R>& kp, bool milne, const ReduceSpec& rs, unsigned long long* hist,
+                               double cut, double width, double* partials, double* obs_out, cudaStream_t st);
+// Fixed-order total of nblocks x kObsNum block partials into out.
+cudaError_t launch_obs_total(const double* partials, int64_t nblocks, double* out, cudaStream_t st);
+
 // Milne (tau, r) sampling tables: the radial acceptance ratio pdf/max_pdf on nbins bin
 // centers and the temperature profile on an ascending r table (linear, clamped).
 struct MilneTables {

@@ -9,6 +9,7 @@
 #include "lim_internal.h"
 #include "lim_step.cuh"
 #include "lim_particle.cuh"
+#include "lim_obs.cuh"
 
 namespace lim {
 
@@ -353,68 +354,28 @@ k_obs_partials(const KParams<R> kp, int from_fo, double cut, double width, doubl
     double v[kObsNum];
 #pragma unroll
     for (int k = 0; k < kObsNum; ++k) v[k] = 0.0;
-    if (i < kp.n) {
-        bool use = true;
-        double p[3] = { 0, 0, 0 }, x[3] = { 0, 0, 0 };
-        if (from_fo) {
-            use = kp.fo_flag[i] != 0.0;
-            for (int d = 0; d < kp.pdim; ++d) p[d] = (double)kp.fo_mom[d][i];
-            for (int d = 0; d < kp.dims; ++d) x[d] = (double)kp.fo_pos[d][i];
-        } else {
-            for (int d = 0; d < kp.pdim; ++d) p[d] = (double)kp.p[d][i];
-            for (int d = 0; d < kp.dims; ++d) {
-                x[d] = (double)kp.x[d][i];
-                if (sizeof(R) == 4) x[d] += (double)kp.xlo[d][i];
-            }
-        }
-        if (use) {
-            const double m = (double)kp.m;
-            double px = p[0], py = kp.pdim >= 2 ? p[1] : 0.0;
-            double pt2 = px * px + py * py, pt = sqrt(pt2);
-            double p2 = 0.0;
-            for (int d = 0; d < kp.pdim; ++d) p2 += p[d] * p[d];
-            double E = sqrt(m * m + p2), w = m / E;
-            v[0] = 1.0;
-            v[1] = pt;
-            v[2] = pt2 > 0.0 ? (px * px - py * py) / pt2 : 0.0;
-            v[3] = pt > cut ? 1.0 : 0.0;
-            v[4] = 1.0 / (1.0 + exp(-(pt - cut) / width));
-            v[5] = p2;
-            v[6] = E;
-            v[7] = w * p2;
-            v[8] = px;
-            v[9] = w * px;
-            v[10] = kp.pdim == 3 ? p[2] * p[2] : 0.0;
-            double x2 = 0.0;
-            for (int d = 0; d < kp.dims; ++d) x2 += x[d] * x[d];
-            v[11] = x2;
-        }
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < kObsNum; ++k) {
-        double a = v[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
-        if (lane == 0) sh[warp][k] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < kObsNum) {
-        double a = 0.0;
-        const int nw = blockDim.x >> 5;
-        for (int w = 0; w < nw; ++w) a += sh[w][threadIdx.x];
-        partials[(int64_t)blockIdx.x * kObsNum + threadIdx.x] = a;
-    }
+    if (i < kp.n) obs_terms<R>(kp, i, from_fo, cut, width, v);
+    obs_block_sum(v, sh, partials + (int64_t)blockIdx.x * kObsNum);
 }
 
-__global__ void k_obs_total(const double* __restrict__ partials, int64_t nblocks, double* __restrict__ out)
+__global__ void __launch_bounds__(kObsNum * 32) k_obs_total(const double* __restrict__ partials, int64_t nblocks,
+                                                             double* __restrict__ out)
 {
-    // one thread per observable, fixed summation order
-    const int k = threadIdx.x;
+    // one warp per observable: lane-strided sums combined by a fixed shuffle tree (a
+    // fixed summation order for a given block count)
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (k >= kObsNum) return;
     double a = 0.0;
-    for (int64_t b = 0; b < nblocks; ++b) a += partials[b * kObsNum + k];
-    out[k] = a;
+    for (int64_t b = lane; b < nblocks; b += 32) a += partials[b * kObsNum + k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+    if (lane == 0) out[k] = a;
+}
+
+cudaError_t launch_obs_total(const double* partials, int64_t nblocks, double* out, cudaStream_t st)
+{
+    k_obs_total<<<1, kObsNum * 32, 0, st>>>(partials, nblocks, out);
+    return cudaGetLastError();
 }
 
 template <typename R>
@@ -424,7 +385,7 @@ cudaError_t launch_observables(const KParams<R>& kp, int from_fo, double cut, do
     const int64_t nb = kp.n == 0 ? 1 : (kp.n + 255) / 256;
     if (nb > nblocks_max) return cudaErrorInvalidValue;
     k_obs_partials<R><<<(unsigned)nb, 256, 0, st>>>(kp, from_fo, cut, width, partials);
-    k_obs_total<<<1, 32, 0, st>>>(partials, nb, out);
+    k_obs_total<<<1, kObsNum * 32, 0, st>>>(partials, nb, out);
     return cudaGetLastError();
 }
 

@@ -5,6 +5,7 @@ hundred thousand particles, inputs above L2, a few GB on the device at most):
   python langevinmedium.jl_b200/profile_cases.py grid    --n 262144 --steps 200 [--fo]
   python langevinmedium.jl_b200/profile_cases.py adjoint --n 262144 --steps 256
   python langevinmedium.jl_b200/profile_cases.py batch   --ensembles 16
+  python langevinmedium.jl_b200/profile_cases.py snapshots --n 1000000 --steps 1880 --save 20
 
 Each prints its device time from the engine's own CUDA events.
 """
@@ -19,7 +20,8 @@ sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["bjorken", "grid", "adjoint", "batch"])
+    ap.add_argument("case", choices=["bjorken", "grid", "adjoint", "batch", "snapshots"])
+    ap.add_argument("--save", type=int, default=20, help="snapshots: steps between saves")
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--fo", action="store_true", help="grid: freeze-out latch, particles stop")
@@ -42,6 +44,18 @@ def main():
         b.run()
         ms, nl, ps = b.stats()
         print(f"batch of {len(wls)}: {ms:.3f} ms, {nl} launches, {ps / (ms * 1e-3):.4g} particle-steps/s")
+        return
+    if a.case == "snapshots":
+        # the Bjorken workload with a snapshot every --save steps, reduced on the device
+        wl = W.bjorken(N=a.n, precision=a.precision, steps=a.steps)
+        e = capi.Engine(0)
+        W.configure(e, wl)
+        e.initial_lab_boost()
+        nslots = wl.steps // a.save + 1
+        spec = capi.reduce_spec(100, 20.0, 100, 10.0)
+        e.run_reduced(wl.first_step, wl.steps, a.save, 0, nslots, spec)
+        ms, nl = e.last_run_stats()
+        print(f"snapshots N={a.n} steps={wl.steps} every {a.save}: {ms:.3f} ms, {nl} launches")
         return
     if a.case == "bjorken":
         wl = W.bjorken(N=a.n, precision=a.precision, steps=a.steps)

@@ -88,7 +88,7 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
                         # additive
                         seed: int = DEFAULT_SEED, precision: str = "fp64", eta_over_s: float = 0.16,
                         tau_R_factor: float = 5.0, device: int = 0, stream=None, block_size: int = 0,
-                        stop_after_freezeout: bool = True):
+                        stop_after_freezeout: bool = True, snapshot_reduce=None):
     mode = _sym(collision_mode)
     if mode not in ("langevin", "rta", "langevin_rta"):
         raise ValueError(f"simulate_ensemble_bulk(::B200Backend): collision_mode=:{mode} is not supported "
@@ -198,6 +198,15 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
         return FreezeOut(fo["pos"], fo["mom"], fo["tau"], fo["flag"])
 
     nslots = num_saves + 1
+    if snapshot_reduce is not None:
+        # additive: every snapshot reduced on the device (observable sums, n(r), p_T
+        # spectrum, cos 2 phi per p_T bin) instead of the FP64 history
+        spec = capi.reduce_spec(*snapshot_reduce)
+        first = eng.reduce_state(spec)
+        rest = eng.run_reduced(1, steps, save_every, 1, nslots - 1, spec) if nslots > 1 else None
+        red = {k: (np.vstack([first[k][None, :], rest[k]]) if rest is not None else first[k][None, :])
+               for k in first}
+        return _time_points(initial_time, final_time, nslots), red
     hx = np.empty(nslots * N * dimensions)
     hp = np.empty(nslots * N * pdim)
     eng.download_state_flat(hx[: N * dimensions], hp[: N * pdim])

@@ -4,6 +4,7 @@ calls that need a GPU fail with a status (no crash) when none is present."""
 import ctypes as C
 import re
 
+import numpy as np
 import pytest
 import torch
 
@@ -46,3 +47,15 @@ def test_oracle_header_and_product_params_agree(lmb, orc):
     a = [f[0] for f in lmb.capi.LimParams._fields_]
     b = [f[0] for f in orc.OrcParams._fields_]
     assert b[:len(a)] == a and b[len(a):] == ["rta_replay"]
+
+
+def test_reduce_stride_on_host(lmb):
+    """lim_reduce_stride is host arithmetic: the per-slot layout of lim_run_reduced."""
+    capi = lmb.capi
+    L = capi.load_library()
+    spec = capi.reduce_spec(64, 16.0, 50, 5.0)
+    assert L.lim_reduce_stride(C.byref(spec)) == capi.LIM_OBS_NUM + 65 + 2 * 51
+    assert L.lim_reduce_stride(C.byref(capi.reduce_spec(0, 16.0, 50, 5.0))) == -1
+    out = np.arange(2 * (capi.LIM_OBS_NUM + 65 + 102), dtype=np.float64)
+    parts = capi.split_reduced(out, spec)
+    assert parts["obs"].shape == (2, capi.LIM_OBS_NUM) and parts["pt_cos2"].shape == (2, 51)
