@@ -160,6 +160,37 @@ int lim_set_medium_grid(lim_ctx* ctx,
 int lim_set_spline(lim_ctx* ctx, int which, double Tmin, double invdT,
                    const double* vals, int64_t n);
 
+/* ---- transport tables built on the device ------------------------------------------
+ * The reference builds its tables on the host (transport.jl:165-365); these entry
+ * points build the same tables on the device (one thread per T node; one block per T
+ * node of the inverse CDF) and install them in the context like lim_set_spline /
+ * lim_set_invcdf, for hosts that configure many ensembles (one spline per D_s variant).
+ *
+ * lim_build_time_spline: vals[i] = time(T_i, m, effective_DsT(T_i)) * scale on
+ * T_i = Tmin + i (Tmax - Tmin)/(nT - 1) into spline `which` (LIM_SPLINE_DRAG or
+ * LIM_SPLINE_RTA), time = tau_drag (transport.jl:132-137, build_tau_drag_spline),
+ * tau_n_main3 (:58-104, build_taun_current_spline) or factor (eta/s)/T (the RTA time of
+ * the Langevin+RTA step; m and D_s unused).  form: effective_DsT's options
+ * (transport.jl:139-156), NULL for a constant D_s; scale: LV_TAUN_SCALE (1 normally).
+ * Errors as the reference's: "nT must be >= 2", "Tmin must be > 0", "Tmax must be > Tmin". */
+enum { LIM_TIME_DRAG = 0, LIM_TIME_TAUN = 1, LIM_TIME_TAUR = 2 };
+typedef struct lim_dsform {
+    int64_t linear;         /* DsT_linear: DsT_slope max(T, Tfo) + DsT_offset */
+    double slope, offset, Tfo;
+    int64_t quad;           /* DsT_quad: DsT (T / DsT_Tref)^2 */
+    double Tref;
+} lim_dsform;
+int lim_build_time_spline(lim_ctx* ctx, int which, int kind, double m, double DsT, const lim_dsform* form,
+                          double Tmin, double Tmax, int64_t nT, double eta_over_s, double factor, double scale);
+/* build_juttner_invcdf (transport.jl:277-365) on the device: T range padded by 2 %,
+ * nT x nU table of the inverse CDF of p^(dims-1) exp(-(E - m)/T) from an np-point
+ * trapezoid CDF, capped at the (1 - quantile_cap) quantile; installed as lim_set_invcdf. */
+int lim_build_juttner_invcdf(lim_ctx* ctx, double m, int64_t dims, double Tmin, double Tmax, int64_t nT, int64_t nU,
+                             int64_t np, double quantile_cap);
+/* The installed tables (n / nU, nT always written; vals when not NULL, cap values). */
+int lim_get_spline(lim_ctx* ctx, int which, double* Tmin, double* invdT, double* vals, int64_t cap, int64_t* n);
+int lim_get_invcdf(lim_ctx* ctx, double* vals, int64_t cap, int64_t* nU, int64_t* nT, double* Tmin, double* invdT);
+
 /* Medium temperature scale s: every medium temperature is s * T (default 1).  No
  * counterpart in the reference; the third parameter of lim_adjoint. */
 int lim_set_medium_scale(lim_ctx* ctx, double s);

@@ -61,6 +61,14 @@ class LimBatchShape(C.Structure):
         return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
+class LimDsForm(C.Structure):
+    _fields_ = [("linear", C.c_int64), ("slope", C.c_double), ("offset", C.c_double), ("Tfo", C.c_double),
+                ("quad", C.c_int64), ("Tref", C.c_double)]
+
+
+LIM_TIME_DRAG, LIM_TIME_TAUN, LIM_TIME_TAUR = 0, 1, 2
+
+
 class LimReduceSpec(C.Structure):
     _fields_ = [("r_bins", C.c_int64), ("r_max", C.c_double), ("pt_bins", C.c_int64), ("pt_max", C.c_double)]
 
@@ -113,6 +121,12 @@ _SIGS = {
     "lim_copy_rta_decisions": ([C.c_void_p, C.c_void_p], C.c_int),
     "lim_adjoint": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
     "lim_adjoint_stats": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_build_time_spline": ([C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(LimDsForm), C.c_double,
+                               C.c_double, C.c_int64, C.c_double, C.c_double, C.c_double], C.c_int),
+    "lim_build_juttner_invcdf": ([C.c_void_p, C.c_double, C.c_int64, C.c_double, C.c_double, C.c_int64, C.c_int64,
+                                  C.c_int64, C.c_double], C.c_int),
+    "lim_get_spline": ([C.c_void_p, C.c_int, _DP, _DP, _DP, C.c_int64, _I64P], C.c_int),
+    "lim_get_invcdf": ([C.c_void_p, _DP, C.c_int64, _I64P, _I64P, _DP, _DP], C.c_int),
     "lim_reduce_stride": ([C.POINTER(LimReduceSpec)], C.c_int64),
     "lim_reduce_state": ([C.c_void_p, C.POINTER(LimReduceSpec), _DP], C.c_int),
     "lim_run_reduced": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.POINTER(LimReduceSpec),
@@ -262,6 +276,41 @@ class Engine:
     def set_spline(self, which, Tmin, invdT, vals):
         v = np.ascontiguousarray(vals, dtype=np.float64)
         self._check(self.lib.lim_set_spline(self.ctx, int(which), float(Tmin), float(invdT), _dptr(v), v.size))
+
+    def build_time_spline(self, which, kind, m, DsT, *, Tmin, Tmax, nT=1024, DsT_linear=False, DsT_slope=1.765,
+                          DsT_offset=-0.159, Tfo=0.156, DsT_quad=False, DsT_Tref=0.0, eta_over_s=0.16,
+                          factor=5.0, scale=None):
+        """A time spline built on the device (lim_build_time_spline); keywords as
+        transport.build_*_spline.  scale defaults to transport.LV_TAUN_SCALE."""
+        from . import transport as _tr
+        form = LimDsForm(int(bool(DsT_linear)), float(DsT_slope), float(DsT_offset), float(Tfo),
+                         int(bool(DsT_quad)), float(DsT_Tref))
+        sc = _tr.LV_TAUN_SCALE if scale is None else float(scale)
+        self._check(self.lib.lim_build_time_spline(self.ctx, int(which), int(kind), float(m), float(DsT),
+                                                   C.byref(form), float(Tmin), float(Tmax), int(nT),
+                                                   float(eta_over_s), float(factor), sc))
+
+    def build_juttner_invcdf(self, m, dimensions, *, Tmin, Tmax, nT=256, nU=2048, np_=8192, quantile_cap=1.0e-6):
+        self._check(self.lib.lim_build_juttner_invcdf(self.ctx, float(m), int(dimensions), float(Tmin), float(Tmax),
+                                                      int(nT), int(nU), int(np_), float(quantile_cap)))
+
+    def get_spline(self, which):
+        """(Tmin, invdT, vals) of the installed spline."""
+        n = C.c_int64(0)
+        t0, inv = C.c_double(0), C.c_double(0)
+        self._check(self.lib.lim_get_spline(self.ctx, int(which), C.byref(t0), C.byref(inv), None, 0, C.byref(n)))
+        vals = np.zeros(max(n.value, 1))
+        self._check(self.lib.lim_get_spline(self.ctx, int(which), None, None, _dptr(vals), vals.size, C.byref(n)))
+        return t0.value, inv.value, vals[:n.value]
+
+    def get_invcdf(self):
+        """(vals, nU, nT, Tmin, invdT) of the installed inverse-CDF table."""
+        nU, nT = C.c_int64(0), C.c_int64(0)
+        t0, inv = C.c_double(0), C.c_double(0)
+        self._check(self.lib.lim_get_invcdf(self.ctx, None, 0, C.byref(nU), C.byref(nT), C.byref(t0), C.byref(inv)))
+        vals = np.zeros(max(nU.value * nT.value, 1))
+        self._check(self.lib.lim_get_invcdf(self.ctx, _dptr(vals), vals.size, None, None, None, None))
+        return vals[:nU.value * nT.value], nU.value, nT.value, t0.value, inv.value
 
     def set_invcdf(self, vals, nU, nT, Tmin, invdT):
         v = np.ascontiguousarray(vals, dtype=np.float64)

@@ -782,6 +782,116 @@ int lim_set_spline(lim_ctx* c, int which, double Tmin, double invdT, const doubl
     return LIM_OK;
 }
 
+int lim_build_time_spline(lim_ctx* c, int which, int kind, double m, double DsT, const lim_dsform* form,
+                          double Tmin, double Tmax, int64_t nT, double eta_over_s, double factor, double scale)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (which < LIM_SPLINE_DRAG || which > LIM_SPLINE_RTA)
+        return fail(c, LIM_ERR_ARG, "lim_build_time_spline: which must be LIM_SPLINE_DRAG or LIM_SPLINE_RTA");
+    if (kind < LIM_TIME_DRAG || kind > LIM_TIME_TAUR) return fail(c, LIM_ERR_ARG, "lim_build_time_spline: unknown kind %d", kind);
+    // transport.jl:165-196 argument checks (and effective_DsT's, :139-156)
+    if (nT < 2) return fail(c, LIM_ERR_ARG, "nT must be >= 2");
+    if (nT > (1 << 24)) return fail(c, LIM_ERR_ARG, "lim_build_time_spline: at most 2^24 nodes");
+    if (!(Tmin > 0.0)) return fail(c, LIM_ERR_ARG, "Tmin must be > 0");
+    if (!(Tmax > Tmin) || !std::isfinite(Tmax)) return fail(c, LIM_ERR_ARG, "Tmax must be > Tmin");
+    TimeSplineSpec sp;
+    std::memset(&sp, 0, sizeof sp);
+    if (form) {
+        if (form->quad && form->linear)
+            return fail(c, LIM_ERR_ARG, "effective_DsT: DsT_quad and DsT_linear are mutually exclusive");
+        if (form->quad && !(form->Tref > 0.0)) return fail(c, LIM_ERR_ARG, "effective_DsT: DsT_quad requires DsT_Tref > 0");
+        sp.linear = form->linear != 0; sp.quad = form->quad != 0;
+        sp.slope = form->slope; sp.offset = form->offset; sp.Tfo = form->Tfo; sp.Tref = form->Tref;
+    }
+    sp.kind = kind; sp.nT = (int)nT; sp.m = m; sp.DsT = DsT; sp.Tmin = Tmin; sp.Tmax = Tmax; sp.scale = scale;
+    sp.eta_over_s = eta_over_s; sp.factor = factor;
+    cudaSetDevice(c->device);
+    DevBuf tmp;
+    int rc = dev_alloc(c, tmp, (size_t)nT * sizeof(double));
+    if (rc) return rc;
+    std::vector<double> vals((size_t)nT);
+    cudaError_t e = launch_time_spline(sp, (double*)tmp.p, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vals.data(), tmp.p, vals.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dev_free(tmp);
+    if (e != cudaSuccess) return fail(c, LIM_ERR_CUDA, "lim_build_time_spline: %s", cudaGetErrorString(e));
+    const double dT = (Tmax - Tmin) / (double)(nT - 1);
+    ++c->gen;
+    c->spl[which] = std::move(vals);
+    c->spl_Tmin[which] = Tmin;
+    c->spl_invdT[which] = 1.0 / dT;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_build_juttner_invcdf(lim_ctx* c, double m, int64_t dims, double Tmin, double Tmax, int64_t nT, int64_t nU,
+                             int64_t np, double quantile_cap)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (nT < 2) return fail(c, LIM_ERR_ARG, "nT must be >= 2");
+    if (nU < 2) return fail(c, LIM_ERR_ARG, "nU must be >= 2");
+    if (np < 2) return fail(c, LIM_ERR_ARG, "np must be >= 2");
+    if (dims < 1 || dims > 3) return fail(c, LIM_ERR_ARG, "lim_build_juttner_invcdf: dimensions must be 1, 2 or 3");
+    if (nT > 65535 || nU > (1 << 24) || np > (1 << 24) || (double)nT * (double)np > 1e9)
+        return fail(c, LIM_ERR_ARG, "lim_build_juttner_invcdf: table too large");
+    // transport.jl:277-300: the T range padded by 2 % on both sides, kept above 1e-4
+    double Tmin_f = std::max(Tmin, 1e-4);
+    double Tmax_f = std::max(Tmax, Tmin_f * (1.0 + 1e-6));
+    const double span = Tmax_f - Tmin_f;
+    Tmin_f = std::max(Tmin_f - 0.02 * span, 1e-4);
+    Tmax_f = Tmax_f + 0.02 * span;
+    JuttnerSpec js;
+    js.dims = (int)dims; js.nT = (int)nT; js.nU = (int)nU; js.np = (int)np;
+    js.m = m; js.Tmin = Tmin_f; js.dT = (Tmax_f - Tmin_f) / (double)(nT - 1); js.quantile_cap = quantile_cap;
+    cudaSetDevice(c->device);
+    DevBuf scratch, inv;
+    int rc = dev_alloc(c, scratch, (size_t)nT * np * sizeof(double));
+    if (!rc) rc = dev_alloc(c, inv, (size_t)nT * nU * sizeof(double));
+    if (rc) { dev_free(scratch); dev_free(inv); return rc; }
+    std::vector<double> vals((size_t)(nT * nU));
+    cudaError_t e = launch_juttner_invcdf(js, (double*)scratch.p, (double*)inv.p, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(vals.data(), inv.p, vals.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dev_free(scratch);
+    dev_free(inv);
+    if (e != cudaSuccess) return fail(c, LIM_ERR_CUDA, "lim_build_juttner_invcdf: %s", cudaGetErrorString(e));
+    ++c->gen;
+    c->icdf = std::move(vals);
+    c->nU = nU; c->nT = nT; c->ic_Tmin = Tmin_f; c->ic_invdT = 1.0 / js.dT;
+    c->dev_dirty = true;
+    return LIM_OK;
+}
+
+int lim_get_spline(lim_ctx* c, int which, double* Tmin, double* invdT, double* vals, int64_t cap, int64_t* n)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (which < LIM_SPLINE_DRAG || which > LIM_SPLINE_DRAG_DB) return fail(c, LIM_ERR_ARG, "lim_get_spline: unknown spline %d", which);
+    const std::vector<double>& v = c->spl[which];
+    if (n) *n = (int64_t)v.size();
+    if (Tmin) *Tmin = c->spl_Tmin[which];
+    if (invdT) *invdT = c->spl_invdT[which];
+    if (vals) {
+        if (cap < (int64_t)v.size()) return fail(c, LIM_ERR_ARG, "lim_get_spline: buffer of %lld values for %zu",
+                                                 (long long)cap, v.size());
+        std::copy(v.begin(), v.end(), vals);
+    }
+    return LIM_OK;
+}
+
+int lim_get_invcdf(lim_ctx* c, double* vals, int64_t cap, int64_t* nU, int64_t* nT, double* Tmin, double* invdT)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (nU) *nU = c->nU;
+    if (nT) *nT = c->nT;
+    if (Tmin) *Tmin = c->ic_Tmin;
+    if (invdT) *invdT = c->ic_invdT;
+    if (vals) {
+        if (cap < (int64_t)c->icdf.size()) return fail(c, LIM_ERR_ARG, "lim_get_invcdf: buffer too small");
+        std::copy(c->icdf.begin(), c->icdf.end(), vals);
+    }
+    return LIM_OK;
+}
+
 int lim_set_medium_scale(lim_ctx* c, double s)
 {
     if (!c) return LIM_ERR_ARG;

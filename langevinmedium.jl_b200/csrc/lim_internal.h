@@ -114,6 +114,22 @@ cudaError_t launch_reduce_hist(const KParams<R>& kp, bool milne, const ReduceSpe
 // Fixed-order total of nblocks x kObsNum block partials into out.
 cudaError_t launch_obs_total(const double* partials, int64_t nblocks, double* out, cudaStream_t st);
 
+// Transport tables built on the device (lim_tables.cu).
+enum { TIME_DRAG = 0, TIME_TAUN = 1, TIME_TAUR = 2 };
+struct TimeSplineSpec {
+    int kind, nT;
+    double m, DsT, Tmin, Tmax, scale;          // scale: LV_TAUN_SCALE
+    int linear, quad;                          // effective_DsT forms (transport.jl:139-156)
+    double slope, offset, Tfo, Tref;
+    double eta_over_s, factor;                 // TIME_TAUR: factor (eta/s) / T
+};
+struct JuttnerSpec {
+    int dims, nT, nU, np;
+    double m, Tmin, dT, quantile_cap;
+};
+cudaError_t launch_time_spline(const TimeSplineSpec& sp, double* vals, cudaStream_t st);
+cudaError_t launch_juttner_invcdf(const JuttnerSpec& js, double* cdf_scratch, double* inv, cudaStream_t st);
+
 // Milne (tau, r) sampling tables: the radial acceptance ratio pdf/max_pdf on nbins bin
 // centers and the temperature profile on an ascending r table (linear, clamped).
 struct MilneTables {

@@ -88,7 +88,7 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
                         # additive
                         seed: int = DEFAULT_SEED, precision: str = "fp64", eta_over_s: float = 0.16,
                         tau_R_factor: float = 5.0, device: int = 0, stream=None, block_size: int = 0,
-                        stop_after_freezeout: bool = True, snapshot_reduce=None):
+                        stop_after_freezeout: bool = True, snapshot_reduce=None, tables: str = "host"):
     mode = _sym(collision_mode)
     if mode not in ("langevin", "rta", "langevin_rta"):
         raise ValueError(f"simulate_ensemble_bulk(::B200Backend): collision_mode=:{mode} is not supported "
@@ -168,7 +168,21 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
                    stop_after_freezeout=int(bool(stop_after_freezeout and freezeout_capture)), block_size=block_size)
     eng.set_medium_rt(xgrid, tgrid, Tfield, Vfield, V2Evolutionn)
     # --- transport tables (simulate_gpu.jl:90-138) ---
-    if momentum_langevin and DsT > 0.0:
+    if tables not in ("host", "device"):
+        raise ValueError('tables must be "host" (transport.py, as the reference) or "device"')
+    if momentum_langevin and DsT > 0.0 and tables == "device":
+        Tmin, Tmax = tr.spline_range(Tfield)
+        dkw = dict(Tmin=Tmin, Tmax=Tmax, nT=1024, DsT_linear=DsT_linear, DsT_slope=DsT_slope,
+                   DsT_offset=DsT_offset, Tfo=Tfo, DsT_quad=DsT_quad, DsT_Tref=DsT_Tref)
+        eng.build_time_spline(capi.LIM_SPLINE_DRAG, capi.LIM_TIME_DRAG, m, DsT, **dkw)
+        if mode == "rta":
+            eng.build_time_spline(capi.LIM_SPLINE_RTA, capi.LIM_TIME_TAUN, m, DsT, **dkw)
+        elif mode == "langevin_rta":
+            eng.build_time_spline(capi.LIM_SPLINE_RTA, capi.LIM_TIME_TAUR, m, DsT, eta_over_s=eta_over_s,
+                                  factor=tau_R_factor, **dkw)
+        if mode in ("rta", "langevin_rta"):
+            eng.build_juttner_invcdf(m, pdim, Tmin=Tmin, Tmax=Tmax, nT=256, nU=2048, np_=8192)
+    elif momentum_langevin and DsT > 0.0:
         Tmin, Tmax = tr.spline_range(Tfield)
         dkw = dict(Tmin=Tmin, Tmax=Tmax, nT=1024, DsT_linear=DsT_linear, DsT_slope=DsT_slope,
                    DsT_offset=DsT_offset, Tfo=Tfo, DsT_quad=DsT_quad, DsT_Tref=DsT_Tref)
