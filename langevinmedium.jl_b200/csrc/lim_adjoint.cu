@@ -153,10 +153,9 @@ __device__ __forceinline__ void adjoint_step(const KParams<float>& kp, int64_t s
     if (col) {
         const uint4 w = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTA);
         const float pstar = invcdf_lookup_dT(kp, w.x, Tk, dpsT);
-        float gv[3], z;
+        float gv[3];
         box_muller(w.y, w.z, gv[0], gv[1]);
-        const uint4 v = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTADIR);
-        box_muller(v.x, v.y, gv[2], z);
+        gv[2] = norm_inv(w.w, 0.0f);
         const float n2 = gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
         const float inv = 1.0f / sqrtf(n2 > 1e-30f ? n2 : 1e-30f);
 #pragma unroll

@@ -123,6 +123,17 @@ int ensure_device_medium(lim_ctx* c)
         if ((rc = upload(c, c->d_tgd, c->tg.data(), nt))) return rc;
         if ((rc = upload(c, c->d_xgd, c->xg.data(), nr))) return rc;
         if ((rc = upload(c, c->d_TV, tv.data(), tv.size()))) return rc;
+        // per-cell records: (T_i, V_i, T_i+1, V_i+1) of each time row, and (x_i, x_i+1)
+        std::vector<R> tvc(4 * (nr - 1) * nt), xc(2 * (nr - 1));
+        for (size_t j = 0; j < nt; ++j)
+            for (size_t i = 0; i + 1 < nr; ++i) {
+                R* q = tvc.data() + 4 * (i + (nr - 1) * j);
+                q[0] = tv[2 * (i + nr * j)]; q[1] = tv[2 * (i + nr * j) + 1];
+                q[2] = tv[2 * (i + 1 + nr * j)]; q[3] = tv[2 * (i + 1 + nr * j) + 1];
+            }
+        for (size_t i = 0; i + 1 < nr; ++i) { xc[2 * i] = xr[i]; xc[2 * i + 1] = xr[i + 1]; }
+        if ((rc = upload(c, c->d_TVc, tvc.data(), tvc.size()))) return rc;
+        if ((rc = upload(c, c->d_xc, xc.data(), xc.size()))) return rc;
         if (!c->V2.empty()) {
             std::vector<R> v2(c->V2.size());
             for (size_t k = 0; k < v2.size(); ++k) v2[k] = (R)c->V2[k];
@@ -209,6 +220,9 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
         md.x_uniform = near_uniform(c->xg, x0, xi); md.xg0 = (R)x0; md.xinvd = (R)xi;
         md.t_uniform = near_uniform(c->tg, t0g, ti); md.tg0 = t0g; md.tinvd = ti;
         md.TV = (const typename V2T<R>::type*)c->d_TV.p;
+        md.TVc = (const typename V4T<R>::type*)c->d_TVc.p;
+        md.xc = (const typename V2T<R>::type*)c->d_xc.p;
+        md.xlo = (R)c->xg.front(); md.xhi = (R)c->xg.back();
         md.V2 = (const R*)c->d_V2.p; md.use_v2 = !c->V2.empty();
         md.r_max = (R)c->xg.back();
         md.r_axis_eps = (R)std::max(1e-12, 0.5 * std::fabs(c->xg[1] - c->xg[0]));
@@ -624,7 +638,7 @@ int lim_destroy(lim_ctx* c)
     if (!c) return LIM_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
+    DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_TVc, &c->d_xc, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
                       &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
                       &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
@@ -655,7 +669,7 @@ int lim_synchronize(lim_ctx* c)
 int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
 {
     if (!c || !bytes) return LIM_ERR_ARG;
-    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
+    const DevBuf* all[] = { &c->d_xg, &c->d_tg, &c->d_tgd, &c->d_xgd, &c->d_TV, &c->d_TVc, &c->d_xc, &c->d_V2, &c->d_G, &c->d_spl[0], &c->d_spl[1], &c->d_spl[2], &c->d_spl[3], &c->d_icdf,
                             &c->d_fo_tau, &c->d_fo_flag, &c->d_l_tau, &c->d_l_T, &c->d_status, &c->d_stage_x, &c->d_stage_p,
                             &c->d_partials, &c->d_obs, &c->d_probe, &c->d_rec, &c->d_steps, &c->d_ckpt,
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,

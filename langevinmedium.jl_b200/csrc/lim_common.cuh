@@ -10,7 +10,7 @@ namespace lim {
 constexpr double kEps = 2.220446049250313e-16;   // Julia eps()
 constexpr double kFmGeV = 1.0 / 0.197327;        // constants.jl:13,23
 constexpr int kNoiseSlots = 11;
-enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4,
+enum { TAG_MOM = 1, TAG_RTA = 2, TAG_DIFF = 4,                   // (tag 3 unused)
        TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6, TAG_SAMPLE_PZ = 7 };   // initial-state sampling (lim_sample.cu)
 enum { MED_RT = 0, MED_BJORKEN = 1, MED_GRID = 2 };
 // The adjoint's tape: float4 rows per particle-step, row k of step s at
@@ -26,6 +26,9 @@ enum { COLL_LANGEVIN = 0, COLL_RTA = 1, COLL_LANGEVIN_RTA = 2, COLL_FLUID = 3 };
 template <typename R> struct V2T;
 template <> struct V2T<double> { using type = double2; };
 template <> struct V2T<float>  { using type = float2; };
+template <typename R> struct V4T;
+template <> struct V4T<double> { using type = double4; };
+template <> struct V4T<float>  { using type = float4; };
 
 // ---------------------------------------------------------------------------
 // Parameter blocks (passed by value to every step kernel)
@@ -38,6 +41,11 @@ struct MediumDev {
     R xg0, xinvd; int x_uniform;                 // O(1) first guess of searchsortedlast
     double tg0, tinvd; int t_uniform;
     const typename V2T<R>::type* TV;
+    // the same table per cell for the step's lookup: TVc[i + (nr-1) j] = (T_i, V_i,
+    // T_i+1, V_i+1) of time row j, xc[i] = (x_i, x_i+1), and the clamp bounds x_0, x_nr-1
+    const typename V4T<R>::type* TVc;
+    const typename V2T<R>::type* xc;
+    R xlo, xhi;
     const R* V2; int use_v2;
     const double* tgd;                           // tgrid in FP64 (time cell is found in FP64)
     const double* xgd;                           // xgrid in FP64 (FP64 freeze-out temperature)

@@ -43,6 +43,7 @@ struct lim_ctx {
     int dev_prec = -1;
     bool dev_dirty = true;
     lim::DevBuf d_xg, d_tg, d_tgd, d_xgd, d_TV, d_V2, d_G, d_spl[4], d_icdf;
+    lim::DevBuf d_TVc, d_xc;              // per-cell (r, t) records for the step's lookup
 
     // particle state (structure of arrays, precision `state_prec`)
     int64_t n = 0;

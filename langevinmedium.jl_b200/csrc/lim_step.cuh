@@ -12,8 +12,7 @@
 //                      xi2 = Phi^-1(u2); RTA decision u_collide = u3 when pdim = 3,
 //                      u2 when pdim < 3, u0 in pure RTA mode           [slots 0-3]
 //   group RTA  (drawn only when a collision happens): u_sample = u0,
-//                      (u1,u2) -> directions g0, g1                    [slots 4-6]
-//   group RTADIR (pdim = 3 collisions): (u0,u1) -> g2                  [slot 7]
+//                      (u1,u2) -> directions g0, g1, g2 = Phi^-1(u3)   [slots 4-7]
 //   group DIFF position-diffusion normals                              [slots 8-10]
 #pragma once
 #include "lim_common.cuh"
@@ -85,25 +84,44 @@ __device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_
 // ---------------------------------------------------------------------------
 // medium lookups
 // ---------------------------------------------------------------------------
-// (r, t) table: bilinear interpolation of (T, V) at radius r (clamped).
+__device__ __forceinline__ float4 ldg_cell(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldg_cell(const double4* p)
+{
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// (r, t) table: bilinear interpolation of (T, V) at radius r (clamped).  The cell is
+// searchsortedlast(x, r) capped to [0, nr-2] (kernels_cpu.jl:22-51): on a near-uniform
+// grid a first guess corrected against the cell's own nodes (one load of xc), else a
+// binary search; the values come from the two per-cell records of time rows kt, kt+1.
 template <typename R>
 __device__ __forceinline__ void rt_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R r, R& T, R& V)
 {
-    R rq = jclamp(r, __ldg(md.xg), __ldg(md.xg + md.nr - 1));
-    int i = cell_index(md.xg, md.nr, rq, md.x_uniform, md.xg0, md.xinvd);
-    R x0 = __ldg(md.xg + i), x1 = __ldg(md.xg + i + 1);
-    R dx = x1 - x0;
-    R xd = fabs(dx) < R(kEps) ? R(0) : (rq - x0) / dx;
-    const int nr = md.nr, j = sr.kt;
-    auto a00 = md.TV[i + nr * j],       a10 = md.TV[i + 1 + nr * j];
-    auto a01 = md.TV[i + nr * (j + 1)], a11 = md.TV[i + 1 + nr * (j + 1)];
-    R yd = sr.wt;
-    R c0 = a00.x * (R(1) - xd) + a10.x * xd;
-    R c1 = a01.x * (R(1) - xd) + a11.x * xd;
-    T = c0 * (R(1) - yd) + c1 * yd;
-    c0 = a00.y * (R(1) - xd) + a10.y * xd;
-    c1 = a01.y * (R(1) - xd) + a11.y * xd;
-    V = c0 * (R(1) - yd) + c1 * yd;
+    const R rq = jclamp(r, md.xlo, md.xhi);
+    const int nc = md.nr - 1;
+    int i;
+    if (md.x_uniform) {
+        const R f = (rq - md.xg0) * md.xinvd;
+        i = f > R(0) ? (int)f : 0;
+        i = i > nc - 1 ? nc - 1 : i;
+    } else {
+        i = cell_index(md.xg, md.nr, rq, 0, md.xg0, md.xinvd);
+    }
+    auto xn = __ldg(md.xc + i);
+    while (i < nc - 1 && xn.y <= rq) xn = __ldg(md.xc + ++i);
+    while (i > 0 && xn.x > rq) xn = __ldg(md.xc + --i);
+    const R dx = xn.y - xn.x;
+    const R xd = fabs(dx) < R(kEps) ? R(0) : (rq - xn.x) / dx;
+    const int j = sr.kt;
+    const auto c0 = ldg_cell(md.TVc + i + nc * j), c1 = ldg_cell(md.TVc + i + nc * (j + 1));
+    const R yd = sr.wt;
+    R a = c0.x * (R(1) - xd) + c0.z * xd;
+    R b = c1.x * (R(1) - xd) + c1.z * xd;
+    T = a * (R(1) - yd) + b * yd;
+    a = c0.y * (R(1) - xd) + c0.w * xd;
+    b = c1.y * (R(1) - xd) + c1.w * xd;
+    V = a * (R(1) - yd) + b * yd;
 }
 
 template <typename R>
@@ -440,12 +458,7 @@ __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int
     R pstar = invcdf_lookup(kp, u.x, T);
     R g[3];
     box_muller(u.y, u.z, g[0], g[1]);
-    g[2] = R(0);
-    if (PDIM == 3) {
-        const uint4 v = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTADIR);
-        R z;
-        box_muller(v.x, v.y, g[2], z);
-    }
+    g[2] = PDIM == 3 ? norm_inv(u.w, R(0)) : R(0);      // one block serves the whole collision
     rec_slot<REC>(kp, s, i, 4, u_exact(u.x));
 #pragma unroll
     for (int d = 0; d < 3; ++d) rec_slot<REC>(kp, s, i, 5 + d, g[d]);

@@ -33,7 +33,7 @@
 
 enum { C_LANGEVIN = 0, C_RTA = 1, C_LANGEVIN_RTA = 2, C_FLUID = 3 };
 enum { M_RT = 0, M_BJORKEN = 1, M_GRID = 2 };
-enum { TAG_MOM = 1, TAG_RTA = 2, TAG_RTADIR = 3, TAG_DIFF = 4, TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6,
+enum { TAG_MOM = 1, TAG_RTA = 2, TAG_DIFF = 4, TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6,
        TAG_SAMPLE_PZ = 7 };
 
 typedef struct orc_params {
@@ -281,7 +281,7 @@ double orc_norm_inv(double p) { return norm_inv(p); }
  * Group MOM: (u0,u1) -> Box-Muller (xi0, xi1); xi2 = Phi^-1(u2) when pdim = 3.  The
  * collision uniform is u3 when pdim = 3, u2 when pdim < 3, and u0 when there is no
  * Langevin kick.  Group RTA (only when a particle collides): u_sample = u0,
- * (u1,u2) -> (g0, g1); group RTADIR: (u0,u1) -> g2. */
+ * (u1,u2) -> (g0, g1), g2 = Phi^-1(u3) when pdim = 3. */
 typedef struct noise_src {
     const double* rec;      /* recorded buffer or NULL (Philox) */
     int64_t rec_first, rec_steps, n;
@@ -319,15 +319,11 @@ static void draw_rta_sample(const orc_params* P, const noise_src* ns, int64_t i,
         for (int k = 0; k < 3; ++k) g[k] = rec_at(ns, i, step, 5 + k);
         return;
     }
-    double u[4], v[4], z;
+    double u[4];
     uniforms4(P, P->particle_offset + i, step, TAG_RTA, u);
     *us = u[0];
     box_muller(u[1], u[2], &g[0], &g[1]);
-    g[2] = 0.0;
-    if (P->pdim == 3) {
-        uniforms4(P, P->particle_offset + i, step, TAG_RTADIR, v);
-        box_muller(v[0], v[1], &g[2], &z);
-    }
+    g[2] = P->pdim == 3 ? norm_inv(u[3]) : 0.0;
 }
 static void draw_diffusion(const orc_params* P, const noise_src* ns, int64_t i, int64_t step, double d[3])
 {
