@@ -168,6 +168,25 @@ def run_reference(args, rank: int, world: int):
 # ---------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------
+def per_pipe_roofline(counts, fma_rate, mufu_rate, particle_steps, kernel_s):
+    """The work model's per-pipe bound (time per particle-step = count / pipe rate, the
+    roofline time the largest of them): FP32 on the FMA pipe and every instruction on
+    issue at the measured FMA rate; MUFU and conversions on the XU pipe at the measured
+    MUFU rate; integer, FP64 and memory instructions at the B200 SM's nominal lane
+    ratios to the FMA pipe (64, 64 and 32 of 128 per clock)."""
+    total = sum(counts.values())
+    rates = {"issue": (total, fma_rate), "fp32": (counts.get("fp32", 0.0), fma_rate),
+             "xu": (counts.get("mufu", 0.0) + counts.get("conv", 0.0), mufu_rate),
+             "int": (counts.get("int", 0.0), fma_rate / 2), "fp64": (counts.get("fp64", 0.0), fma_rate / 2),
+             "mem": (counts.get("mem", 0.0), fma_rate / 4)}
+    t = {k: c / r for k, (c, r) in rates.items()}
+    bound = max(t, key=t.get)
+    return {"time_per_particle_step_ns": {k: v * 1e9 for k, v in t.items()}, "bound": bound,
+            "frac": t[bound] * particle_steps / kernel_s,
+            "rates_thread_instr_per_s": {k: r for k, (c, r) in rates.items()},
+            "note": "XU count includes the conversions; ALU/FP64/LSU rates nominal ratios of the measured FMA rate"}
+
+
 def work_model(pkg):
     wm = json.loads((Path(pkg.__file__).parent / "work_model.json").read_text())
     w = wm["workloads"]["bjorken_langevin_rta_fp32"]
@@ -315,12 +334,16 @@ def bench_adjoint(pkg, args):
     }
 
 
-def bench_grid(pkg, args, fma_rate):
+def bench_grid(pkg, args, fma_rate, mufu_rate):
     """The 2+1D grid workload: 5e6 charm + 5e6 bottom, freeze-out at T < 0.155 GeV
     (particles stop when they freeze out), 940 steps of 0.01 fm."""
     W, capi = pkg.workloads, pkg.capi
     wm = json.loads((Path(pkg.__file__).parent / "work_model.json").read_text())
-    i_alg = sum(sum(v.values()) for v in wm["workloads"]["grid2p1_langevin_rta_fo_fp32"]["items"].values())
+    counts = {}
+    for item in wm["workloads"]["grid2p1_langevin_rta_fo_fp32"]["items"].values():
+        for k, c in item.items():
+            counts[k] = counts.get(k, 0.0) + c
+    i_alg = sum(counts.values())
     fields = W.grid2p1_fields()
     tot_ms, executed, nominal = 0.0, 0.0, 0
     reps = max(1, min(args.steps, 3))
@@ -352,7 +375,8 @@ def bench_grid(pkg, args, fma_rate):
         "executed_particle_steps": executed, "nominal_particle_steps": nominal, "kernel_ms": tot_ms,
         "roofline": {"bound": "issue", "unit": "Ginst/s", "algorithmic_inst_per_particle_step": i_alg,
                      "achieved": i_alg * rate / 1e9, "peak": fma_rate / 1e9, "frac": i_alg * rate / fma_rate,
-                     "peak_source": "FP32 FMA issue probe (lim_probe_fma_rate), this run"},
+                     "peak_source": "FP32 FMA issue probe (lim_probe_fma_rate), this run",
+                     "per_pipe": per_pipe_roofline(counts, fma_rate, mufu_rate, executed, tot_ms * 1e-3)},
         "timing": f"CUDA events of the runs (table, step and compaction kernels), median of {reps} after one warm-up",
     }
 
@@ -464,6 +488,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # ---- roofline of the step kernel ----
     counts, i_alg, hbm_pp = work_model(pkg)
     fma_rate, _ = eng.probe_fma_rate()                    # measured FP32 issue ceiling (thread-instr/s)
+    mufu_rate, _ = eng.probe_mufu_rate()                  # measured XU ceiling
     kern_s = (total_kern_ms / args.steps) * 1e-3
     achieved = i_alg * ps_per_pass / kern_s               # algorithmic thread-instructions per second
     bytes_launch = hbm_pp * n
@@ -476,6 +501,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "inst_mix_per_particle_step": counts,
         "peak_source": "measured in this run: FP32 FMA issue probe (lim_probe_fma_rate), thread-instr/s",
         "kernel_ms_per_launch": kern_s * 1e3,
+        "per_pipe": per_pipe_roofline(counts, fma_rate, mufu_rate, ps_per_pass, kern_s),
         "hbm": {"algorithmic_bytes_per_launch": bytes_launch, "achieved_gbs": bytes_launch / kern_s / 1e9,
                 "peak_gbs": 6544.3, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
     }
@@ -492,7 +518,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if world == 1 and not args.quick:
         extra["batched"] = bench_batched(pkg, args, flush)
         extra["adjoint"] = bench_adjoint(pkg, args)
-        extra["grid2p1"] = bench_grid(pkg, args, fma_rate)
+        extra["grid2p1"] = bench_grid(pkg, args, fma_rate, mufu_rate)
     elif world > 1:
         extra["batched"] = extra["adjoint"] = extra["grid2p1"] = {"skipped": "measured in the one-GPU run"}
     if rank == 0:

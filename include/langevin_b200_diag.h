@@ -18,6 +18,11 @@ extern "C" {
  * measured with CUDA events on the context stream; ms is the probe duration. */
 int lim_probe_fma_rate(lim_ctx* ctx, double* thread_fma_per_s, double* ms);
 
+/* Issue rate of independent hardware-exponential (ex2.approx) chains over the whole
+ * GPU: thread-level multi-function-unit instructions per second, the ceiling of the
+ * transcendental / conversion (XU) pipe; measured like lim_probe_fma_rate. */
+int lim_probe_mufu_rate(lim_ctx* ctx, double* thread_mufu_per_s, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

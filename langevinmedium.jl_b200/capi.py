@@ -114,6 +114,7 @@ _SIGS = {
     "lim_philox_device": ([C.c_void_p, _U32P, _U32P, _U32P], C.c_int),
     "lim_last_run_stats": ([C.c_void_p, _DP, _I64P], C.c_int),
     "lim_probe_fma_rate": ([C.c_void_p, _DP, _DP], C.c_int),
+    "lim_probe_mufu_rate": ([C.c_void_p, _DP, _DP], C.c_int),
     "lim_observables_noalloc": ([C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int64, C.c_double,
                                  C.c_double, C.c_double, C.c_void_p, C.c_void_p], C.c_int),
     "lim_set_medium_scale": ([C.c_void_p, C.c_double], C.c_int),
@@ -450,6 +451,13 @@ class Engine:
         r = C.c_double(0.0)
         ms = C.c_double(0.0)
         self._check(self.lib.lim_probe_fma_rate(self.ctx, C.byref(r), C.byref(ms)))
+        return r.value, ms.value
+
+    def probe_mufu_rate(self):
+        """(thread MUFU instructions per second, probe ms) of the XU-pipe probe."""
+        r = C.c_double(0.0)
+        ms = C.c_double(0.0)
+        self._check(self.lib.lim_probe_mufu_rate(self.ctx, C.byref(r), C.byref(ms)))
         return r.value, ms.value
 
     def device_bytes(self) -> int:

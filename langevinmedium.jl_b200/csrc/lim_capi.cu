@@ -1450,6 +1450,27 @@ int lim_probe_fma_rate(lim_ctx* c, double* thread_fma_per_s, double* ms_out)
     return LIM_OK;
 }
 
+int lim_probe_mufu_rate(lim_ctx* c, double* thread_mufu_per_s, double* ms_out)
+{
+    if (!c || !thread_mufu_per_s) return LIM_ERR_ARG;
+    cudaSetDevice(c->device);
+    int nsm = 0;
+    LIM_CUDA(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    const int blocks = nsm * 8, iters = 512;
+    int rc = dev_alloc(c, c->d_probe, (size_t)blocks * 256 * sizeof(float));
+    if (rc) return rc;
+    LIM_CUDA(c, launch_mufu_probe((float*)c->d_probe.p, blocks, 16, c->stream));   // warm-up
+    LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    LIM_CUDA(c, launch_mufu_probe((float*)c->d_probe.p, blocks, iters, c->stream));
+    LIM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    LIM_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    LIM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *thread_mufu_per_s = (double)blocks * 256.0 * iters * 64.0 / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return LIM_OK;
+}
+
 int lim_last_run_stats(lim_ctx* c, double* kernel_ms, int64_t* launches)
 {
     if (!c) return LIM_ERR_ARG;

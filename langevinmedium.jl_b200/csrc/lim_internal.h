@@ -146,6 +146,8 @@ cudaError_t launch_philox_probe(const uint32_t* ctr_key, uint32_t* out, cudaStre
 
 // FP32 FMA issue-rate probe: `blocks` x 256 threads, 64 FMAs per thread per iteration.
 cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st);
+// XU (MUFU) issue-rate probe: `blocks` x 256 threads, 64 ex2.approx per thread per iteration.
+cudaError_t launch_mufu_probe(float* out, int blocks, int iters, cudaStream_t st);
 
 // Message returned by lim_last_error(NULL) for entry points that take no context.
 void set_noctx_error(const char* msg);

@@ -411,6 +411,37 @@ cudaError_t launch_fma_probe(float* out, int blocks, int iters, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Multi-function-unit (XU) probe: 8 independent chains of the hardware base-2
+// exponential (ex2.approx, one MUFU instruction each) with one FP32 multiply to keep the
+// values bounded; the XU pipe, with an eighth of the FMA pipe's lanes, is the bound.
+__global__ void __launch_bounds__(256) k_mufu_probe(float* out, int iters, float b)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = -1e-3f * (float)(threadIdx.x + k);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float e;
+                asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(a[k]));
+                a[k] = -b * e;
+            }
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launch_mufu_probe(float* out, int blocks, int iters, cudaStream_t st)
+{
+    k_mufu_probe<<<blocks, 256, 0, st>>>(out, iters, 0.5f);
+    return cudaGetLastError();
+}
+
 __global__ void k_philox_probe(const uint32_t* ck, uint32_t* out)
 {
     uint4 r = philox4x32_10(make_uint4(ck[0], ck[1], ck[2], ck[3]), make_uint2(ck[4], ck[5]));
