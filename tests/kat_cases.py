@@ -7,6 +7,7 @@ from __future__ import annotations
 import math
 
 import numpy as np
+from scipy import special
 
 from helpers import HBARC_TEST, K2K3, est, juttner_sample, lam1, p2eq
 
@@ -33,6 +34,17 @@ def case_equilibria(box_run):
     assert math.isclose(e2["lam"], lam1(M_, T_, 2), rel_tol=0.005)
     assert e2["lam"] / e3["lam"] > 1.06
     assert math.isclose(np.mean(m3[-1][2] ** 2), np.mean(m3[-1][0] ** 2), rel_tol=0.02)
+    # the ensemble means against the Jüttner values within 3 standard errors:
+    # <E> = m K1(z)/K2(z) + 3T in 3-D, (m^2 + 2mT + 2T^2)/(m + T) in 2-D (z = m/T)
+    z = M_ / T_
+    e_eq = {3: M_ * special.kv(1, z) / special.kv(2, z) + 3 * T_, 2: (M_ ** 2 + 2 * M_ * T_ + 2 * T_ ** 2) / (M_ + T_)}
+    for P, d in ((m3[-1], 3), (m2[-1], 2)):
+        p2 = np.sum(P ** 2, axis=0)
+        E = np.sqrt(M_ ** 2 + p2)
+        for name, v, ref in (("<p^2>", p2, p2eq(M_, T_, d)), ("<E>", E, e_eq[d])):
+            dev = (np.mean(v) - ref) / (np.std(v) / math.sqrt(v.size))
+            print(f"equilibrium d={d} {name}: {np.mean(v) / ref - 1:+.4%} = {dev:+.2f} standard errors")
+            assert abs(dev) < 3.0
     return e3, e2
 
 
@@ -63,6 +75,8 @@ def case_l1_decay(box_run, N_D=200_000):
         c = np.linalg.lstsq(A, np.log(jx), rcond=None)[0]
         rates[d] = -c[1]
         refs[d] = (K2K3(M_ / T_) if d == 3 else lam1(M_, T_, d)) * ETA_
+        print(f"l=1 decay d={d}: fitted rate {rates[d] / refs[d] - 1:+.3%}, instantaneous {r_inst / refs[d] - 1:+.3%} "
+              f"against eta_D lambda_1")
         assert math.isclose(r_inst, refs[d], rel_tol=0.012)
         assert math.isclose(rates[d], refs[d], rel_tol=0.04)
     assert rates[2] / rates[3] > 1.05
@@ -93,6 +107,7 @@ def case_msd(box_run):
     A = np.vstack([np.ones(sel.sum()), tt[sel]]).T
     c = np.linalg.lstsq(A, msd[sel], rcond=None)[0]
     Ds_meas = c[1] / 4
+    print(f"MSD: D_s {Ds_meas / DS_FM - 1:+.3%} against DsT/T")
     assert math.isclose(Ds_meas, DS_FM, rel_tol=0.03)
     return Ds_meas
 
