@@ -120,9 +120,34 @@ def cpu_sample(pkg, n_particles: int, threads: int = 0, calib_steps: int = 0):
     md.invcdf(*wl.invcdf)
     x0, p0 = orc.initial_lab_boost(P, md, wl.x, wl.p)
     t = time.perf_counter()
-    orc.run(P, md, x0, p0, wl.first_step, steps, threads=threads)
+    out = orc.run(P, md, x0, p0, wl.first_step, steps, threads=threads)
     dt = time.perf_counter() - t
-    return n_particles * steps / dt, dict(particles=n_particles, steps=steps, seconds=dt)
+    return n_particles * steps / dt, dict(particles=n_particles, steps=steps, seconds=dt, x=out["x"], p=out["p"])
+
+
+def accuracy_against_cpu_sample(pkg, n_particles: int, info: dict) -> dict:
+    """The engine in FP32 and FP64 on the particles of the timed CPU sample, against
+    that sample's FP64 final state (same Philox noise): per particle
+    ||a - b|| / max(||b||, floor * scale), scale 0.3 GeV for momenta and 1 fm for
+    positions, floor 1e-2 in FP64 and 1 in FP32 (the parity tests' metric)."""
+    W, capi = pkg.workloads, pkg.capi
+    out = {"sample": f"{n_particles} charm quarks x 1880 steps (the CPU sample's particles)",
+           "metric": "per-particle relative error, max and 99.99th percentile"}
+    for prec, floor in (("fp64", 1e-2), ("fp32", 1.0)):
+        wl = W.bjorken(N=n_particles, precision=prec, rng_seed=2)
+        e = capi.Engine(0)
+        W.configure(e, wl)
+        e.initial_lab_boost()
+        e.run(wl.first_step, wl.steps)
+        x, p = e.download_state()
+        e.close()
+        res = {}
+        for name, a, b, sc in (("p", p, info["p"], 0.3), ("x", x, info["x"], 1.0)):
+            err = np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), floor * sc)
+            res[f"{name}_max"] = float(err.max())
+            res[f"{name}_p9999"] = float(np.percentile(err, 99.99))
+        out[f"{prec}_vs_fp64_cpu"] = res
+    return out
 
 
 def size_cpu_sample(pkg, target_s: float, threads: int) -> int:
@@ -505,7 +530,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "hbm": {"algorithmic_bytes_per_launch": bytes_launch, "achieved_gbs": bytes_launch / kern_s / 1e9,
                 "peak_gbs": 6544.3, "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
     }
-    cpu = None
+    cpu = accuracy = None
     if rank == 0 and not args.no_cpu_baseline:
         from oracle import oracle as orc
         threads = orc.max_threads()
@@ -514,6 +539,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                "sample": f"{ncpu} charm quarks x 1880 steps of the same workload, FP64 restatement (oracle/), "
                          f"{info['seconds']:.1f} s"}
+        accuracy = accuracy_against_cpu_sample(pkg, ncpu, info)
     extra = {}
     if world == 1 and not args.quick:
         extra["batched"] = bench_batched(pkg, args, flush)
@@ -536,6 +562,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "gpu_launches": launches,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "clocks": clk,
             "observables": {k: float(v) for k, v in zip(capi.OBS_NAMES, (sums.cpu().numpy() /
                                                                        max(float(sums[0]), 1.0)))},
