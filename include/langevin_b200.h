@@ -108,7 +108,8 @@ typedef struct lim_params {
     int64_t seed;               /* Philox-4x32-10 key (64 bit) */
     int64_t particle_offset;    /* global id of particle 0 (shards keep the global noise stream) */
     int64_t stop_after_freezeout; /* 1: stop evolving a particle once latched (fo outputs unchanged) */
-    int64_t block_size;         /* threads per block of the step kernel; 0 = autotuned default */
+    int64_t block_size;         /* threads per block of the step kernel, a multiple of 32 up to 256;
+                                   0 = the measured default (128 or 256 by kernel) */
 } lim_params;
 
 typedef struct lim_ctx lim_ctx;

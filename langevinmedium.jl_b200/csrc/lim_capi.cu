@@ -276,11 +276,18 @@ int check_ready(lim_ctx* c)
     return LIM_OK;
 }
 
+// Threads per block of the step kernels: the caller's choice, else 128 for the FP32
+// Cartesian kernels of the (r, t) and Bjorken media and for the grid with freeze-out
+// (1 % faster than 256 on the benchmark workloads: the same residency in finer blocks
+// balances the last wave), 256 for the rest (the grid without freeze-out measured 0.7 %
+// faster at 256).
 int block_of(const lim_ctx* c)
 {
     int b = (int)c->P.block_size;
-    if (b <= 0) b = 256;
-    return b;
+    if (b > 0) return b;
+    const bool fp32_cart = c->P.precision == LIM_FP32 && c->P.coords == LIM_COORDS_CARTESIAN;
+    if (fp32_cart && (c->med_kind != MED_GRID || c->P.freezeout_capture)) return 128;
+    return 256;
 }
 
 constexpr int64_t kLiveSteps = 32;   // steps between compactions of the live list
@@ -718,8 +725,8 @@ int lim_set_params(lim_ctx* c, const lim_params* P)
     if (q.integrator_mode != 0 && q.integrator_mode != 1)
         return fail(c, LIM_ERR_ARG, "integrator_mode must be 0 or 1");
     if (q.precision != LIM_FP64 && q.precision != LIM_FP32) return fail(c, LIM_ERR_ARG, "precision must be LIM_FP64 or LIM_FP32");
-    if (q.block_size < 0 || q.block_size > 1024 || (q.block_size % 32) != 0)
-        return fail(c, LIM_ERR_ARG, "block_size must be a multiple of 32 in [32, 1024] (or 0)");
+    if (q.block_size < 0 || q.block_size > 256 || (q.block_size % 32) != 0)
+        return fail(c, LIM_ERR_ARG, "block_size must be a multiple of 32 in [32, 256] (or 0)");
     // A state of another shape or precision, or without latch buffers (they are
     // allocated at upload), no longer matches: it is dropped and must be uploaded again.
     const bool stale = c->have_state &&
