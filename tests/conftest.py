@@ -31,7 +31,13 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def lmb():
-    return load_pkg()
+    pkg = load_pkg()
+    if not pkg.capi.LIB_PATH.exists():          # a fresh checkout: build the in-tree library first
+        spec = importlib.util.spec_from_file_location("_lim_build", PKG_DIR / "build.py")
+        b = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(b)
+        b.build()
+    return pkg
 
 
 @pytest.fixture(scope="session")
