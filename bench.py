@@ -359,6 +359,28 @@ def bench_adjoint(pkg, args):
     }
 
 
+def bench_fp64(pkg, args):
+    """The headline workload in FP64 (the same 1e6 charm x 1880 steps), for the
+    configuration's FP64 run: CUDA events, median of 3 after one warm-up."""
+    W, capi = pkg.workloads, pkg.capi
+    wl = W.bjorken(N=args.particles, precision="fp64", rng_seed=2)
+    e = capi.Engine(0)
+    W.configure(e, wl)
+    e.initial_lab_boost()
+    e.state_save()
+    ms = []
+    for r in range(4):
+        e.state_restore()
+        e.run(wl.first_step, wl.steps)
+        if r:
+            ms.append(e.last_run_stats()[0])
+    e.close()
+    t = statistics.median(ms)
+    return {"workload": WORKLOAD.replace("fp32", "fp64"), "unit": "particle-steps/s",
+            "value": wl.n * wl.steps / (t * 1e-3), "ms_per_pass": t,
+            "timing": "CUDA events of the run (table and step kernels), median of 3 after one warm-up"}
+
+
 def bench_grid(pkg, args, fma_rate, mufu_rate):
     """The 2+1D grid workload: 5e6 charm + 5e6 bottom, freeze-out at T < 0.155 GeV
     (particles stop when they freeze out), 940 steps of 0.01 fm."""
@@ -545,8 +567,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         extra["batched"] = bench_batched(pkg, args, flush)
         extra["adjoint"] = bench_adjoint(pkg, args)
         extra["grid2p1"] = bench_grid(pkg, args, fma_rate, mufu_rate)
+        extra["fp64"] = bench_fp64(pkg, args)
     elif world > 1:
-        extra["batched"] = extra["adjoint"] = extra["grid2p1"] = {"skipped": "measured in the one-GPU run"}
+        extra["batched"] = extra["adjoint"] = extra["grid2p1"] = extra["fp64"] = {"skipped": "measured in the one-GPU run"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
