@@ -7,7 +7,10 @@
  * are analytic and statistical), so trajectory-level parity is pinned against
  * the reference's own known-answer tests (transport identities, Bjorken
  * telescoping to 1e-9, OU/Jüttner equilibria, l=1 decay, MSD, relativistic
- * switch), which this restatement passes in tests/test_oracle_kats.py.
+ * switch), which this restatement passes in tests/test_oracle_kats.py.  The restated
+ * initial-state samplers (orc_sample_fonll, orc_sample_milne) are pinned by the
+ * reference's p_z test and by distribution tests against utils.jl's CDF construction
+ * (tests/test_sample_oracle.py).
  *
  * Every function follows the Julia source line by line (paths relative to the
  * reference project); compile with -O2 -ffp-contract=off because Julia does not
