@@ -10,7 +10,7 @@ sweep once; backward contracts the incoming cotangent with the 3 x 3 Jacobian it
 returned.  The noise (counter-based, keyed by seed, particle and step) and the RTA
 collision indicators of the forward pass are held fixed, so the gradient is the
 pathwise derivative of the sampled ensemble.  The Julia counterpart is the
-ChainRulesCore rule in julia/LangevInB200ChainRulesExt.jl.
+ChainRulesCore rule in julia/ext/LangevInB200ChainRulesExt.jl.
 """
 from __future__ import annotations
 

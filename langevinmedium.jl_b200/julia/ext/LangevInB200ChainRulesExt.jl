@@ -6,14 +6,15 @@ returns (⟨pT⟩, ⟨cos 2φ⟩, smoothed fraction above the cut) of a configur
 θ = (a, b, s) — 2πT·D_s = a + b(max(T, Tc)/Tc − 1) and the medium temperature scale s —
 and its `rrule` runs the engine's checkpointed forward and hand-written reverse sweep
 (`lim_adjoint`) once, the pullback contracting the cotangent with the 3×3 Jacobian.
-The noise and the RTA indicators of the forward pass are held fixed. Load after
-`LangevInB200` when ChainRulesCore is available (Zygote, Diffractor and the like use it).
+The noise and the RTA indicators of the forward pass are held fixed. A package
+extension of LangevInB200 (Project.toml), loaded with ChainRulesCore (which Zygote,
+Diffractor and the like use).
 """
 module LangevInB200ChainRulesExt
 
 using ChainRulesCore
 using LangevInMedium
-using ..LangevInB200: Ctx, check, libpath, set_spline
+using LangevInB200: Ctx, check, libpath, set_spline
 const LM = LangevInMedium
 
 """A configured context (parameters, medium, RTA spline, inverse CDF, initial state

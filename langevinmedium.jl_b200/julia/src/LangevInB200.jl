@@ -26,7 +26,8 @@ export B200Backend, B200_GCBackend
 struct B200Backend <: LM.Backends.AbstractBackend end
 struct B200_GCBackend <: LM.Backends.AbstractBackend end
 
-const libpath = Ref{String}(joinpath(@__DIR__, "..", "liblangevin_b200.so"))
+# the in-tree library, built by __graft_entry__.build() (langevinmedium.jl_b200/liblangevin_b200.so)
+const libpath = Ref{String}(joinpath(@__DIR__, "..", "..", "liblangevin_b200.so"))
 
 # ---- the C-ABI parameter block: 8 Float64 then 16 Int64, as lim_params -------------------
 struct LimParams
