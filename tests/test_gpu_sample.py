@@ -173,3 +173,36 @@ def test_milne_run_from_device_sample(lmb, orc):
     assert np.max(np.abs(pos[0][0] - xo[1])) <= 1e-12 * 10
     assert np.max(np.abs(mom[0] - po[1])) <= 1e-12 * 10
     assert len(mom) == 3 and np.all(np.isfinite(mom[-1])) and np.all(np.isfinite(pos[-1]))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_grid_freezeout_run_from_device_sample(lmb, orc, prec):
+    """Device FONLL sample (with thermal p_z from the grid medium at tau0), then the 2+1D
+    grid Langevin+RTA run with the freeze-out latch and stopping particles, against the
+    oracle started from its own sample: the latched outputs agree and the same particles
+    freeze out."""
+    from helpers import oracle_medium, oracle_params
+    r, p, f = fonll_like()
+    fields = lmb.workloads.grid2p1_fields(nx=81, ny=61, nt=24, dx=0.25)
+    n, steps = 2048, 300
+    wl = lmb.workloads.grid2p1(N=n, precision=prec, fields=fields, steps=steps, dt=0.02)
+    e = lmb.capi.Engine(0)
+    lmb.workloads.configure(e, wl, upload=False)
+    e.sample_fonll(r, p, f, n, cartesian=True, thermal_pz=True)
+    e.initial_lab_boost()
+    e.run(1, steps)
+    fo = e.download_freezeout()
+    P = oracle_params(orc, wl)
+    md = oracle_medium(orc, wl)
+    xo, po, failed = orc.sample_fonll(P, md, r, p, f, n, cartesian=True, thermal_pz=True)
+    assert failed == 0
+    x0, p0 = orc.initial_lab_boost(P, md, xo, po)
+    out = orc.run(P, md, x0, p0, 1, steps)
+    assert np.array_equal(fo["flag"], out["fo_flag"])
+    assert np.count_nonzero(fo["flag"]) > 0
+    for a, b, sc in ((fo["mom"], out["fo_mom"], 0.3), (fo["pos"], out["fo_pos"], 1.0)):
+        emax, e99 = parity(a, b, sc, 1e-2 if prec == "fp64" else 1.0)
+        if prec == "fp64":
+            assert emax <= 1e-12, emax
+        else:
+            assert e99 <= 1e-5 and emax <= 1e-3, (emax, e99)
