@@ -265,6 +265,14 @@ int lim_reduce_state(lim_ctx* ctx, const lim_reduce_spec* spec, double* out);
 int lim_run_reduced(lim_ctx* ctx, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
                     int64_t nslots, const lim_reduce_spec* spec, double* out);
 
+/* Page-locked host memory for snapshot histories (and any other host buffer of the
+ * engine): lim_run copies each snapshot on a copy stream while the next interval's
+ * steps run, at the full host-link rate when hist_x / hist_p lie in page-locked memory
+ * (about 3x the rate into pageable memory).  Allocate once and reuse: locking pages
+ * costs time of its own.  No counterpart in the reference. */
+int lim_host_alloc(int64_t bytes, void** out);
+int lim_host_free(void* ptr);
+
 /* First step at which a particle became non-finite, or -1. */
 int lim_status(lim_ctx* ctx, int64_t* first_bad_step);
 

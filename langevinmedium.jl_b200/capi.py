@@ -77,6 +77,33 @@ def reduce_spec(r_bins: int, r_max: float, pt_bins: int, pt_max: float) -> LimRe
     return LimReduceSpec(int(r_bins), float(r_max), int(pt_bins), float(pt_max))
 
 
+class _PinnedBlock:
+    """Owner of one lim_host_alloc block; freed when the last array viewing it goes."""
+
+    def __init__(self, lib, nbytes: int):
+        self.lib, self.ptr = lib, C.c_void_p()
+        rc = lib.lim_host_alloc(int(nbytes), C.byref(self.ptr))
+        if rc != LIM_OK:
+            raise LimError(rc, lib.lim_last_error(None).decode())
+
+    def __del__(self):
+        if self.ptr and self.ptr.value:
+            self.lib.lim_host_free(self.ptr)
+            self.ptr = C.c_void_p()
+
+
+def pinned_empty(n: int, dtype=np.float64, lib: C.CDLL | None = None) -> np.ndarray:
+    """An uninitialised 1-D array of n elements in page-locked host memory
+    (lim_host_alloc): snapshot histories written into it move at the host-link rate."""
+    lib = lib or load_library()
+    dt = np.dtype(dtype)
+    n = int(n)
+    block = _PinnedBlock(lib, max(n, 1) * dt.itemsize)
+    raw = (C.c_char * (max(n, 1) * dt.itemsize)).from_address(block.ptr.value)
+    raw._owner = block                       # the ctypes view keeps the block alive
+    return np.frombuffer(raw, dtype=dt, count=n)
+
+
 def split_reduced(out: np.ndarray, spec: LimReduceSpec) -> dict:
     """(nslots, stride) doubles of lim_run_reduced / lim_reduce_state -> named arrays."""
     nr, npt = int(spec.r_bins) + 1, int(spec.pt_bins) + 1
@@ -128,6 +155,8 @@ _SIGS = {
                                   C.c_int64, C.c_double], C.c_int),
     "lim_get_spline": ([C.c_void_p, C.c_int, _DP, _DP, _DP, C.c_int64, _I64P], C.c_int),
     "lim_get_invcdf": ([C.c_void_p, _DP, C.c_int64, _I64P, _I64P, _DP, _DP], C.c_int),
+    "lim_host_alloc": ([C.c_int64, C.POINTER(C.c_void_p)], C.c_int),
+    "lim_host_free": ([C.c_void_p], C.c_int),
     "lim_reduce_stride": ([C.POINTER(LimReduceSpec)], C.c_int64),
     "lim_reduce_state": ([C.c_void_p, C.POINTER(LimReduceSpec), _DP], C.c_int),
     "lim_run_reduced": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.POINTER(LimReduceSpec),

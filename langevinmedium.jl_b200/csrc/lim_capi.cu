@@ -310,6 +310,23 @@ int reduce_snapshot(lim_ctx* c, const KParams<R>& kp, const SnapshotReduce& red,
     return LIM_OK;
 }
 
+// Copies the snapshot staged in buffer b (once its staging kernels have run) into slot
+// `slot` of the host history, on the copy stream; the host waits for the copy, while
+// the compute stream goes on with the next interval.
+int copy_snapshot(lim_ctx* c, int b, int64_t slot, double* hist_x, double* hist_p, DevBuf* const* stage_x,
+                  DevBuf* const* stage_p)
+{
+    LIM_CUDA(c, cudaStreamWaitEvent(c->copy_stream, c->ev_snap[b], 0));
+    if (hist_x)
+        LIM_CUDA(c, cudaMemcpyAsync(hist_x + slot * c->n * c->dims, stage_x[b]->p, sizeof(double) * c->n * c->dims,
+                                    cudaMemcpyDeviceToHost, c->copy_stream));
+    if (hist_p)
+        LIM_CUDA(c, cudaMemcpyAsync(hist_p + slot * c->n * c->pdim, stage_p[b]->p, sizeof(double) * c->n * c->pdim,
+                                    cudaMemcpyDeviceToHost, c->copy_stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->copy_stream));
+    return LIM_OK;
+}
+
 template <typename R>
 int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
              double* hist_x, double* hist_p, const SnapshotReduce* red = nullptr)
@@ -333,6 +350,22 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
         if ((rc = dev_alloc(c, c->d_live[0], (size_t)c->n * sizeof(int)))) return rc;
         if ((rc = dev_alloc(c, c->d_live[1], (size_t)c->n * sizeof(int)))) return rc;
         if ((rc = dev_alloc(c, c->d_live_n, 2 * sizeof(unsigned)))) return rc;
+    }
+    // snapshot staging: two buffers, copied to the host on the copy stream
+    const bool to_host = saving && !red;
+    DevBuf* stage_x[2] = { &c->d_stage_x, &c->d_stage2_x };
+    DevBuf* stage_p[2] = { &c->d_stage_p, &c->d_stage2_p };
+    int sb = 0;
+    int64_t pending = -1;                  // slot staged in buffer 1 - sb, not yet copied
+    if (to_host) {
+        if (!c->copy_stream) LIM_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : c->ev_snap)
+            if (!e) LIM_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        const size_t nn = (size_t)std::max<int64_t>(c->n, 1);
+        for (int b = 0; b < 2; ++b) {
+            if ((rc = dev_alloc(c, *stage_x[b], nn * c->dims * sizeof(double)))) return rc;
+            if ((rc = dev_alloc(c, *stage_p[b], nn * c->pdim * sizeof(double)))) return rc;
+        }
     }
     LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     int64_t s = first_step;
@@ -377,25 +410,26 @@ int run_impl(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every,
         } else if (saving && last % save_every == 0 && last >= 0) {
             const int64_t slot = last / save_every - first_slot;
             if (slot >= 0) {
+                // stage the snapshot (SoA -> the Julia layout) in buffer sb and copy the
+                // previous one to the host while this interval's successor runs
                 R* xs[3] = { kp.x[0], kp.x[1], kp.x[2] };
                 double* ps[3] = { kp.p[0], kp.p[1], kp.p[2] };
-                if (hist_x) {
+                if (hist_x)
                     LIM_CUDA(c, launch_soa_to_aos<R>(xs, sizeof(R) == 4 ? kp.xlo : nullptr, c->dims, c->n,
-                                                     (double*)c->d_stage_x.p, c->stream));
-                    LIM_CUDA(c, cudaMemcpyAsync(hist_x + slot * c->n * c->dims, c->d_stage_x.p,
-                                                sizeof(double) * c->n * c->dims, cudaMemcpyDeviceToHost, c->stream));
-                }
-                if (hist_p) {
-                    LIM_CUDA(c, launch_soa_to_aos<double>(ps, nullptr, c->pdim, c->n, (double*)c->d_stage_p.p, c->stream));
-                    LIM_CUDA(c, cudaMemcpyAsync(hist_p + slot * c->n * c->pdim, c->d_stage_p.p,
-                                                sizeof(double) * c->n * c->pdim, cudaMemcpyDeviceToHost, c->stream));
-                }
+                                                     (double*)stage_x[sb]->p, c->stream));
+                if (hist_p)
+                    LIM_CUDA(c, launch_soa_to_aos<double>(ps, nullptr, c->pdim, c->n, (double*)stage_p[sb]->p, c->stream));
+                LIM_CUDA(c, cudaEventRecord(c->ev_snap[sb], c->stream));
                 launches += 2;
+                if (pending >= 0 && (rc = copy_snapshot(c, 1 - sb, pending, hist_x, hist_p, stage_x, stage_p))) return rc;
+                pending = slot;
+                sb = 1 - sb;
             }
         }
         s = chunk_end;
     }
     LIM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if (pending >= 0 && (rc = copy_snapshot(c, 1 - sb, pending, hist_x, hist_p, stage_x, stage_p))) return rc;
     LIM_CUDA(c, cudaEventSynchronize(c->ev1));
     float ms = 0.f;
     LIM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
@@ -651,7 +685,7 @@ int lim_destroy(lim_ctx* c)
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
                       &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
-                      &c->d_red_obs, &c->d_red_hist };
+                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -659,6 +693,8 @@ int lim_destroy(lim_ctx* c)
     }
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (cudaEvent_t e : c->ev_snap) if (e) cudaEventDestroy(e);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return LIM_OK;
@@ -682,7 +718,7 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
                       &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
-                      &c->d_red_obs, &c->d_red_hist };
+                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -1362,6 +1398,32 @@ int lim_run_reduced(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save
                                    : run_impl<double>(c, first_step, nsteps, save_every, first_slot, nullptr, nullptr, &red);
     if (rc) return rc;
     return reduce_download(c, red, out);
+}
+
+int lim_host_alloc(int64_t bytes, void** out)
+{
+    if (!out || bytes < 0) {
+        lim::set_noctx_error("lim_host_alloc: need a size >= 0 and an output pointer");
+        return LIM_ERR_ARG;
+    }
+    *out = nullptr;
+    if (bytes == 0) return LIM_OK;
+    const cudaError_t e = cudaHostAlloc(out, (size_t)bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        lim::set_noctx_error((std::string("lim_host_alloc: cudaHostAlloc failed: ") + cudaGetErrorString(e)).c_str());
+        return LIM_ERR_NOMEM;
+    }
+    return LIM_OK;
+}
+
+int lim_host_free(void* ptr)
+{
+    if (ptr && cudaFreeHost(ptr) != cudaSuccess) {
+        lim::set_noctx_error("lim_host_free: cudaFreeHost failed");
+        return LIM_ERR_CUDA;
+    }
+    return LIM_OK;
 }
 
 int lim_status(lim_ctx* c, int64_t* first_bad_step)

@@ -69,6 +69,11 @@ struct lim_ctx {
     uint64_t gen = 0;
 
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // snapshot copies to the host overlap the next interval's steps: a copy stream, two
+    // staging buffers (d_stage_* and d_stage2_*) and their "staged" events (made on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_snap[2] = { nullptr, nullptr };
+    lim::DevBuf d_stage2_x, d_stage2_p;
     double last_ms = 0.0;
     int64_t last_launches = 0;
 };

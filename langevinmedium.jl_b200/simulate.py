@@ -88,7 +88,8 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
                         # additive
                         seed: int = DEFAULT_SEED, precision: str = "fp64", eta_over_s: float = 0.16,
                         tau_R_factor: float = 5.0, device: int = 0, stream=None, block_size: int = 0,
-                        stop_after_freezeout: bool = True, snapshot_reduce=None, tables: str = "host"):
+                        stop_after_freezeout: bool = True, snapshot_reduce=None, tables: str = "host",
+                        pinned_history: bool = False):
     mode = _sym(collision_mode)
     if mode not in ("langevin", "rta", "langevin_rta"):
         raise ValueError(f"simulate_ensemble_bulk(::B200Backend): collision_mode=:{mode} is not supported "
@@ -221,8 +222,11 @@ def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,
         red = {k: (np.vstack([first[k][None, :], rest[k]]) if rest is not None else first[k][None, :])
                for k in first}
         return _time_points(initial_time, final_time, nslots), red
-    hx = np.empty(nslots * N * dimensions)
-    hp = np.empty(nslots * N * pdim)
+    # additive: pinned_history puts the history in page-locked memory (faster copies,
+    # slower to allocate)
+    alloc = capi.pinned_empty if pinned_history else np.empty
+    hx = alloc(nslots * N * dimensions)
+    hp = alloc(nslots * N * pdim)
     eng.download_state_flat(hx[: N * dimensions], hp[: N * pdim])
     eng.run(1, steps, save_every, 0, hx, hp)
     time_points = _time_points(initial_time, final_time, nslots)

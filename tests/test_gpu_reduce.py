@@ -137,3 +137,21 @@ def test_simulate_with_snapshot_reduce(lmb):
         rc, pc, cs = reduce_np(pos[k], mom[k], SPEC)
         assert np.array_equal(red["r_counts"][k], rc) and np.array_equal(red["pt_counts"][k], pc)
         assert np.array_equal(red["pt_cos2"][k], cs)
+
+
+def test_history_in_pinned_memory(lmb):
+    """lim_run's snapshot copies into page-locked buffers (lim_host_alloc) give the same
+    history as into pageable ones."""
+    xg, tg, Tf, Vf = box_medium(0.3, 0.0, 2.0)
+    rng = np.random.default_rng(6)
+    n = 5000
+    kw = dict(N_particles=n, Δt=0.01, initial_time=0.0, final_time=0.6, save_interval=0.1, m=1.5, DsT=0.3,
+              dimensions=2, Tfo=0.0, seed=12, x_init=rng.normal(0, 3, (2, n)), p_init=rng.normal(0, 1, (2, n)))
+    args = (lmb.B200Backend(), xg, np.linspace(0, 10, 10), np.ones((xg.size, 10)), Tf, Vf, (xg, tg))
+    _, m0, x0 = lmb.simulate_ensemble_bulk(*args, **kw)
+    _, m1, x1 = lmb.simulate_ensemble_bulk(*args, pinned_history=True, **kw)
+    assert len(m0) == 7 and all(np.array_equal(a, b) for a, b in zip(m0, m1))
+    assert all(np.array_equal(a, b) for a, b in zip(x0, x1))
+    buf = lmb.capi.pinned_empty(10)
+    buf[:] = np.arange(10)
+    assert buf.sum() == 45 and lmb.capi.pinned_empty(0).size == 0
