@@ -5,7 +5,7 @@ hundred thousand particles, inputs above L2, a few GB on the device at most):
   python langevinmedium.jl_b200/profile_cases.py grid    --n 262144 --steps 200 [--fo]
   python langevinmedium.jl_b200/profile_cases.py adjoint --n 262144 --steps 256
   python langevinmedium.jl_b200/profile_cases.py batch   --ensembles 16
-  python langevinmedium.jl_b200/profile_cases.py snapshots --n 1000000 --steps 1880 --save 20
+  python langevinmedium.jl_b200/profile_cases.py snapshots --n 1000000 --steps 1880 --save 20 [--compare]
 
 Each prints its device time from the engine's own CUDA events.
 """
@@ -22,6 +22,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["bjorken", "grid", "adjoint", "batch", "snapshots"])
     ap.add_argument("--save", type=int, default=20, help="snapshots: steps between saves")
+    ap.add_argument("--compare", action="store_true",
+                    help="snapshots: also time no snapshots and the host history (pageable and page-locked)")
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--fo", action="store_true", help="grid: freeze-out latch, particles stop")
@@ -53,9 +55,31 @@ def main():
         e.initial_lab_boost()
         nslots = wl.steps // a.save + 1
         spec = capi.reduce_spec(100, 20.0, 100, 10.0)
-        e.run_reduced(wl.first_step, wl.steps, a.save, 0, nslots, spec)
-        ms, nl = e.last_run_stats()
-        print(f"snapshots N={a.n} steps={wl.steps} every {a.save}: {ms:.3f} ms, {nl} launches")
+        if not a.compare:
+            e.run_reduced(wl.first_step, wl.steps, a.save, 0, nslots, spec)
+            ms, nl = e.last_run_stats()
+            print(f"snapshots N={a.n} steps={wl.steps} every {a.save}: {ms:.3f} ms, {nl} launches")
+            return
+        # wall-clock of the whole call (the copies are part of it), median of 3 after a warm-up
+        import time
+        import numpy as np
+        e.state_save()
+        size = nslots * a.n
+        page = (np.zeros(size * 2), np.zeros(size * 3))
+        pinned = (capi.pinned_empty(size * 2), capi.pinned_empty(size * 3))
+        cases = {"none": lambda: e.run(wl.first_step, wl.steps),
+                 "reduced": lambda: e.run_reduced(wl.first_step, wl.steps, a.save, 0, nslots, spec),
+                 "history, page-locked": lambda: e.run(wl.first_step, wl.steps, a.save, 0, *pinned),
+                 "history, pageable": lambda: e.run(wl.first_step, wl.steps, a.save, 0, *page)}
+        for name, fn in cases.items():
+            ts = []
+            for r in range(4):
+                e.state_restore()
+                t = time.perf_counter()
+                fn()
+                if r:
+                    ts.append(1e3 * (time.perf_counter() - t))
+            print(f"{name}: {np.median(ts):.1f} ms ({nslots} snapshots, {size * 40 / 1e9:.2f} GB of history)")
         return
     if a.case == "bjorken":
         wl = W.bjorken(N=a.n, precision=a.precision, steps=a.steps)
