@@ -1,5 +1,5 @@
 """The reference's dynamical known-answer tests on the CPU restatement (the oracle):
-this pins the oracle to the reference's own assertions before it is used to judge
+this pins the oracle to the reference's own assertions before it is used to check
 the CUDA engine.  CPU only (OpenMP)."""
 import math
 
