@@ -65,6 +65,16 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     }
     const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
+    // FP32 grid runs with the freeze-out latch: one spatial lookup per step, at the end
+    // of the step for the next step's time row, serves both the next step and the
+    // latch's screen.  The first step's rows are looked up here; every step then takes
+    // its medium from the same code whether or not a launch boundary falls before it,
+    // so a run split into more launches gives the same bits.
+    constexpr bool kCarry = FO && MED == MED_GRID && sizeof(R) == 4;
+    GridRows<R> rows;
+    rows.kt = -1;
+    GridRows<R>* carry = kCarry ? &rows : nullptr;
+    if (kCarry && s0 < s1) grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows);
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && flag != 0.0) break;
         const StepRec<R> sr = tab[s];
@@ -73,8 +83,14 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             *t = make_float4((float)x[0], (float)x[1], (float)p[0], (float)p[1]);
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];
         }
-        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
-        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT);
+        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, carry);
+        if constexpr (kCarry) {
+            // the next step's time row: from the table inside the launch, computed past it
+            double w;
+            const int kn = s + 1 < s1 ? tab[s + 1].kt : grid_time_cell(kp.med, step_time(kp, s + 1), w);
+            grid_rows(kp.med, kn, x[0], x[1], rows);
+        }
+        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT, carry);
         if (!state_finite<R, DIMS, PDIM>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;

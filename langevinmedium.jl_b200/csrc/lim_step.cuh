@@ -38,11 +38,30 @@ struct __align__(16) StepRec {
 
 enum { MED_MILNE_TABLE = 3 };   // Milne (tau, r): unclamped time interpolation
 
+// t0 + s dt, rounded in this order wherever a step's time is needed
+template <typename R>
+__device__ __forceinline__ double step_time(const KParams<R>& kp, int64_t s)
+{
+    return __dadd_rn(__dmul_rn((double)s, kp.dt), kp.t0);
+}
+
+// The 2+1D grid's time cell of time t (clamped to the grid): the row kt and the weight.
+template <typename R>
+__device__ __forceinline__ int grid_time_cell(const MediumDev<R>& md, double t, double& w)
+{
+    const double tq = t > md.gtl ? md.gtl : (t < md.gt0 ? md.gt0 : t);
+    const double f = (tq - md.gt0) / md.gdt_d;
+    const double fl = floor(f);
+    const int it = fl < 0.0 ? 0 : (fl > (double)(md.gnt - 2) ? md.gnt - 2 : (int)fl);
+    w = f - (double)it;
+    return it;
+}
+
 template <typename R, int MED>
 __device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_t s)
 {
     StepRec<R> u;
-    u.t = __dadd_rn(__dmul_rn((double)s, kp.dt), kp.t0);
+    u.t = step_time(kp, s);
     u.tR = (R)u.t;
     u.kt = 0; u.wt = R(0); u.T_bj = R(0); u.zf = 1.0; u.wtd = 0.0; u.Td = 0.0;
     const MediumDev<R>& md = kp.med;
@@ -66,12 +85,7 @@ __device__ __forceinline__ StepRec<R> make_step_rec(const KParams<R>& kp, int64_
         u.T_bj = (R)T;
         u.Td = T;
     } else {
-        double tq = u.t > md.gtl ? md.gtl : (u.t < md.gt0 ? md.gt0 : u.t);
-        double f = (tq - md.gt0) / md.gdt_d;
-        double fl = floor(f);
-        int it = fl < 0.0 ? 0 : (fl > (double)(md.gnt - 2) ? md.gnt - 2 : (int)fl);
-        u.kt = it;
-        u.wtd = f - (double)it;
+        u.kt = grid_time_cell(md, u.t, u.wtd);
         u.wt = (R)u.wtd;
     }
     if (kp.redshift) {                 // kernels_cpu.jl:427-435
@@ -150,12 +164,81 @@ __device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, in
     R y = yq > (R)md.gyl_d ? (R)md.gyl_d : (yq < (R)md.gy0_d ? (R)md.gy0_d : yq);
     R fx, fy;
     if (sizeof(R) == 8) { fx = (x - (R)md.gx0_d) / (R)md.gdx_d; fy = (y - (R)md.gy0_d) / (R)md.gdy_d; }
-    else { fx = (x - (R)md.gx0_d) * (R)md.ginvdx; fy = (y - (R)md.gy0_d) * (R)md.ginvdy; }
+    else { fx = __fmul_rn(x - (R)md.gx0_d, (R)md.ginvdx); fy = __fmul_rn(y - (R)md.gy0_d, (R)md.ginvdy); }
     R flx = floor(fx), fly = floor(fy);
     ix = flx < R(0) ? 0 : (flx > R(md.gnx - 2) ? md.gnx - 2 : (int)flx);
     iy = fly < R(0) ? 0 : (fly > R(md.gny - 2) ? md.gny - 2 : (int)fly);
     wx = fx - R(ix);
     wy = fy - R(iy);
+}
+
+// a (1 - w) + b w as one product and one fused multiply-add, the rounding spelled out:
+// the compiler may not contract it differently where it is inlined, so the grid's
+// interpolation gives the same bits in every kernel and at every call site.
+__device__ __forceinline__ float lerp_rn(float a, float b, float w)
+{
+    return __fmaf_rn(b, w, __fmul_rn(a, __fsub_rn(1.0f, w)));
+}
+__device__ __forceinline__ double lerp_rn(double a, double b, double w)
+{
+    return __fma_rn(b, w, __dmul_rn(a, __dsub_rn(1.0, w)));
+}
+template <typename R>
+__device__ __forceinline__ R bilerp_rn(float a00, float a10, float a01, float a11, R wx, R wy)
+{
+    return lerp_rn(lerp_rn((R)a00, (R)a10, wx), lerp_rn((R)a01, (R)a11, wx), wy);
+}
+
+// The grid at a position, interpolated in space only: (T, v^x, v^y) on time rows kt
+// (T0, U0, V0) and kt + 1 (T1, U1, V1), the two values grid_lookup blends in time.  The
+// freeze-out kernel looks them up once per step, at the end of step s for the time row
+// of step s + 1 at the new position: step s + 1 takes its medium from them, and the
+// latch of step s its temperature screen when the two steps share the time row.
+template <typename R>
+struct GridRows {
+    R T0, T1, U0, U1, V0, V1;
+    int kt;
+};
+
+// The 2 x 2 x 2 grid nodes around (xq, yq) on time rows kt (a) and kt + 1 (b), in the
+// order 00, 10, 01, 11 (x fastest), and the cell weights.
+template <typename R>
+__device__ __forceinline__ void grid_corners(const MediumDev<R>& md, int kt, R xq, R yq, float4 (&a)[4],
+                                             float4 (&b)[4], R& Wx, R& Wy)
+{
+    int ix, iy;
+    grid_cell(md, xq, yq, ix, iy, Wx, Wy);
+    const float4* s0 = md.G + ((size_t)kt * md.gny + iy) * md.gnx + ix;
+    const float4* s1 = s0 + (size_t)md.gny * md.gnx;
+    a[0] = __ldg(s0); a[1] = __ldg(s0 + 1); a[2] = __ldg(s0 + md.gnx); a[3] = __ldg(s0 + md.gnx + 1);
+    b[0] = __ldg(s1); b[1] = __ldg(s1 + 1); b[2] = __ldg(s1 + md.gnx); b[3] = __ldg(s1 + md.gnx + 1);
+}
+
+template <typename R>
+__device__ __forceinline__ void rows_of(const float4 (&a)[4], const float4 (&b)[4], R Wx, R Wy, GridRows<R>& g)
+{
+    g.T0 = bilerp_rn(a[0].x, a[1].x, a[2].x, a[3].x, Wx, Wy); g.T1 = bilerp_rn(b[0].x, b[1].x, b[2].x, b[3].x, Wx, Wy);
+    g.U0 = bilerp_rn(a[0].y, a[1].y, a[2].y, a[3].y, Wx, Wy); g.U1 = bilerp_rn(b[0].y, b[1].y, b[2].y, b[3].y, Wx, Wy);
+    g.V0 = bilerp_rn(a[0].z, a[1].z, a[2].z, a[3].z, Wx, Wy); g.V1 = bilerp_rn(b[0].z, b[1].z, b[2].z, b[3].z, Wx, Wy);
+}
+
+template <typename R>
+__device__ __forceinline__ void grid_rows(const MediumDev<R>& md, int kt, R xq, R yq, GridRows<R>& g)
+{
+    float4 a[4], b[4];
+    R Wx, Wy;
+    grid_corners(md, kt, xq, yq, a, b, Wx, Wy);
+    rows_of(a, b, Wx, Wy, g);
+    g.kt = kt;
+}
+
+// (T, v^x, v^y) at time weight Wt between the rows
+template <typename R>
+__device__ __forceinline__ void grid_combine(const GridRows<R>& g, R Wt, R& T, R& ux, R& uy)
+{
+    T = lerp_rn(g.T0, g.T1, Wt);
+    ux = lerp_rn(g.U0, g.U1, Wt);
+    uy = lerp_rn(g.V0, g.V1, Wt);
 }
 
 // The grid medium at the particle with its gradient in (x, y) (zero along an axis where
@@ -168,25 +251,16 @@ template <typename R, bool GRAD = false>
 __device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R xq, R yq, R& T, R& ux, R& uy,
                                             MedGrad* mg = nullptr)
 {
-    int ix, iy;
+    float4 a[4], b[4];
     R Wx, Wy;
-    grid_cell(md, xq, yq, ix, iy, Wx, Wy);
+    grid_corners(md, sr.kt, xq, yq, a, b, Wx, Wy);
     const R Wt = sr.wt;
-    const float4* s0 = md.G + ((size_t)sr.kt * md.gny + iy) * md.gnx + ix;
-    const float4* s1 = s0 + (size_t)md.gny * md.gnx;
-    float4 a00 = __ldg(s0), a10 = __ldg(s0 + 1), a01 = __ldg(s0 + md.gnx), a11 = __ldg(s0 + md.gnx + 1);
-    float4 b00 = __ldg(s1), b10 = __ldg(s1 + 1), b01 = __ldg(s1 + md.gnx), b11 = __ldg(s1 + md.gnx + 1);
-#define LIM_BILERP(c, A00, A10, A01, A11)                                              \
-    ((((R)A00.c) * (R(1) - Wx) + ((R)A10.c) * Wx) * (R(1) - Wy) +                          \
-     (((R)A01.c) * (R(1) - Wx) + ((R)A11.c) * Wx) * Wy)
-    R T0 = LIM_BILERP(x, a00, a10, a01, a11), T1 = LIM_BILERP(x, b00, b10, b01, b11);
-    R U0 = LIM_BILERP(y, a00, a10, a01, a11), U1 = LIM_BILERP(y, b00, b10, b01, b11);
-    R V0 = LIM_BILERP(z, a00, a10, a01, a11), V1 = LIM_BILERP(z, b00, b10, b01, b11);
-#undef LIM_BILERP
-    T = T0 * (R(1) - Wt) + T1 * Wt;
-    ux = U0 * (R(1) - Wt) + U1 * Wt;
-    uy = V0 * (R(1) - Wt) + V1 * Wt;
+    GridRows<R> g;
+    rows_of(a, b, Wx, Wy, g);
+    grid_combine(g, Wt, T, ux, uy);
     if constexpr (GRAD) {
+        const float4 &a00 = a[0], &a10 = a[1], &a01 = a[2], &a11 = a[3];
+        const float4 &b00 = b[0], &b10 = b[1], &b01 = b[2], &b11 = b[3];
         const float wx = (float)Wx, wy = (float)Wy, wt = (float)Wt;
         const float kx = (xq > (R)md.gx0_d && xq < (R)md.gxl_d) ? md.ginvdx : 0.0f;
         const float ky = (yq > (R)md.gy0_d && yq < (R)md.gyl_d) ? md.ginvdy : 0.0f;
@@ -219,7 +293,7 @@ struct Local {
 
 template <typename R, int MED, int DIMS, bool GRAD = false>
 __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
-                                                 MedGrad* mg = nullptr)
+                                                 MedGrad* mg = nullptr, GridRows<R>* carry = nullptr)
 {
     constexpr bool fp32 = sizeof(R) == 4;
     Local<R> L;
@@ -227,7 +301,11 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     if (MED == MED_GRID) {
         // the grid holds the flow velocity (v^x, v^y), as the reference's (r, t) tables do
         R ux, uy;
-        grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg);
+        if (!GRAD && carry) {                 // the rows of this step's time row at x
+            grid_combine(*carry, sr.wt, L.T, ux, uy);
+        } else {
+            grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg);
+        }
         R u = sqrt(ux * ux + uy * uy);
         L.boost = !(u < R(kEps));
         L.v = u;
@@ -627,7 +705,8 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
 // One Cartesian step (simulate_cpu.jl:215-290).
 template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
-                                          const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
+                                          const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3],
+                                          GridRows<R>* carry = nullptr)
 {
     // the grid medium's tape rows 0, 2, 3 (pre-step momentum, medium and gradient); row 1
     // (the normals and v^x) follows the kick
@@ -635,7 +714,7 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
     MedGrad mg;
     float4* trow = nullptr;
     if constexpr (kTapeGrid) trow = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 4 * kp.n + i;
-    const Local<R> L = local_medium<R, MED, DIMS, kTapeGrid>(kp, sr, x, &mg);
+    const Local<R> L = local_medium<R, MED, DIMS, kTapeGrid>(kp, sr, x, &mg, carry);
     if constexpr (kTapeGrid) {
         trow[0] = make_float4((float)p[0], (float)p[1], (float)p[2], mg.T);
         trow[2 * kp.n] = make_float4(mg.vy, mg.dT[0], mg.dT[1], mg.dvx[0]);
@@ -771,12 +850,7 @@ __device__ __forceinline__ StepRec<R> step_rec_at_time(const KParams<R>& kp, dou
     } else if (MED == MED_BJORKEN) {
         u.Td = (t > md.bj_tau0) ? md.bj_T0 * pow(md.bj_tau0 / t, md.bj_power) : md.bj_T0;
     } else {
-        double tq = t > md.gtl ? md.gtl : (t < md.gt0 ? md.gt0 : t);
-        double f = (tq - md.gt0) / md.gdt_d;
-        double fl = floor(f);
-        int it = fl < 0.0 ? 0 : (fl > (double)(md.gnt - 2) ? md.gnt - 2 : (int)fl);
-        u.kt = it;
-        u.wtd = f - (double)it;
+        u.kt = grid_time_cell(md, t, u.wtd);
     }
     return u;
 }
@@ -822,7 +896,7 @@ template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
                                                 const R (&x)[3], const float (&xl)[3], const double (&p)[3],
                                                 double& flag, double (&lpos)[3], double (&lmom)[3],
-                                                double& ltau, double& lT)
+                                                double& ltau, double& lT, GridRows<R>* carry = nullptr)
 {
     constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
     if (flag != 0.0) return;
@@ -840,7 +914,13 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
             r = sqrt(r2); }
         T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
     } else {
-        const float Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
+        float Ts;
+        if (MED == MED_GRID && carry) {      // the next step's rows at the new position
+            // (no screen where the next step starts a new time row: the FP64 test decides)
+            Ts = carry->kt == sr.kt ? (float)lerp_rn(carry->T0, carry->T1, sr.wt) * (float)kp.med.T_scale : -1.0f;
+        } else {
+            Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
+        }
         if (Ts >= (float)Tfo + kScreen) {            // clearly above: remember the step only
 #pragma unroll
             for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
