@@ -54,10 +54,11 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     double p[3];
     float xl[3];
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    double flag = 0.0, ltau = 0.0, lT = 0.0;
+    bool frozen = false;
+    double ltau = 0.0, lT = 0.0;
     double lpos[3] = { 0.0, 0.0, 0.0 }, lmom[3] = { 0.0, 0.0, 0.0 };
     if (FO) {
-        flag = kp.fo_flag[i]; ltau = kp.l_tau[i]; lT = kp.l_T[i];
+        frozen = kp.fo_flag[i] != 0.0; ltau = kp.l_tau[i]; lT = kp.l_T[i];
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
 #pragma unroll
@@ -76,7 +77,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     GridRows<R>* carry = kCarry ? &rows : nullptr;
     if (kCarry && s0 < s1) grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows);
     for (int64_t s = s0; s < s1; ++s) {
-        if (FO && kp.stop_fo && flag != 0.0) break;
+        if (FO && kp.stop_fo && frozen) break;
         const StepRec<R> sr = tab[s];
         if (REC == 2 && MED != MED_GRID) {   // the adjoint's tape: the pre-step state (the normals follow)
             float4* t = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 2 * kp.n + i;
@@ -90,7 +91,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             const int kn = s + 1 < s1 ? tab[s + 1].kt : grid_time_cell(kp.med, step_time(kp, s + 1), w);
             grid_rows(kp.med, kn, x[0], x[1], rows);
         }
-        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, flag, lpos, lmom, ltau, lT, carry);
+        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, frozen, lpos, lmom, ltau, lT, carry);
         if (!state_finite<R, DIMS, PDIM>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;

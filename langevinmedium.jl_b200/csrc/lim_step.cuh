@@ -895,11 +895,11 @@ __device__ __forceinline__ float temperature_screen(const KParams<R>& kp, const 
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
                                                 const R (&x)[3], const float (&xl)[3], const double (&p)[3],
-                                                double& flag, double (&lpos)[3], double (&lmom)[3],
+                                                bool& frozen, double (&lpos)[3], double (&lmom)[3],
                                                 double& ltau, double& lT, GridRows<R>* carry = nullptr)
 {
     constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
-    if (flag != 0.0) return;
+    if (frozen) return;
     double xd[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (sizeof(R) == 4 ? (double)xl[d] : 0.0);
@@ -944,7 +944,7 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom[d] + frac * (p[d] - lmom[d]);
         kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
         kp.fo_flag[i] = 1.0;
-        flag = 1.0;
+        frozen = true;
     } else {
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
