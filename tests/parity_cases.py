@@ -49,7 +49,7 @@ def initial(rng, N, dims, pdim, spread=4.0, pmax=4.0):
 
 CASES = ["static3d", "flow2d", "flow2d_nonrel", "flow2d_v2", "flow2d_midpoint", "flow2d_nonuniform",
          "flow3d", "rta2d", "lrta_bjorken_table", "fluid_redshift", "radial_diffusion_reflect",
-         "cart_diffusion_reflect", "freezeout", "milne", "bjorken_analytic", "grid_lrta_fo"]
+         "cart_diffusion_reflect", "freezeout", "milne", "bjorken_analytic", "grid_lrta_fo", "grid_fine_tau_fo"]
 
 
 def build_case(name: str, precision: str = "fp64", N: int = 2048, steps: int | None = None, seed: int = 7):
@@ -115,5 +115,11 @@ def build_case(name: str, precision: str = "fp64", N: int = 2048, steps: int | N
     if name == "grid_lrta_fo":
         f = W.grid2p1_fields(nx=81, ny=61, nt=24, dx=0.25, sx=3.0, sy=2.4)
         wl = W.grid2p1(N=N, precision=precision, fields=f, steps=steps or 300, seed=seed, dt=0.02)
+        return wl
+    if name == "grid_fine_tau_fo":
+        # time rows (dtau 0.0151) finer than the step (0.02): every step starts a new
+        # time row, so the FP32 kernel's latch screen never reuses the step's lookup
+        f = W.grid2p1_fields(nx=41, ny=41, nt=160, dx=0.5, tau0=0.6, tauf=3.0, sx=3.0, sy=2.4)
+        wl = W.grid2p1(N=N, precision=precision, fields=f, steps=steps or 110, seed=seed, dt=0.02)
         return wl
     raise KeyError(name)

@@ -100,7 +100,7 @@ def test_fp32_parity_recorded_noise(lmb, orc, name):
     check_fo_outputs(lmb, orc, wl, name, record=True)
 
 
-@pytest.mark.parametrize("name", ["static3d", "lrta_bjorken_table", "grid_lrta_fo", "milne"])
+@pytest.mark.parametrize("name", ["static3d", "lrta_bjorken_table", "grid_lrta_fo", "grid_fine_tau_fo", "milne"])
 def test_fp32_parity_philox(lmb, orc, name):
     """FP32 engine vs FP64 restatement regenerating the FP32 uniforms from Philox
     (the whole FP32 error: arithmetic plus the FP32 noise transform)."""
@@ -251,14 +251,15 @@ def test_observables_match_host_reduction(lmb):
     assert np.isclose(obs["mean_p2"], np.mean(np.sum(p ** 2, axis=0)), rtol=1e-12)
 
 
-def test_live_list_run_matches_full_grid_run(lmb):
+@pytest.mark.parametrize("name,steps", [("grid_lrta_fo", 200), ("grid_fine_tau_fo", 110)])
+def test_live_list_run_matches_full_grid_run(lmb, name, steps):
     """Runs that stop particles at freeze-out advance a compacted list of the live
     particles; the result equals the run over every particle (the noise-recording
     instantiation takes that path), latch outputs included, and the run split into two
     calls (the FP32 kernel carries the grid lookup of one step into the next, so a launch
     boundary must not change the bits)."""
     for prec in ("fp32", "fp64"):
-        wl = build_case("grid_lrta_fo", prec, N=20000, steps=200)
+        wl = build_case(name, prec, N=20000, steps=steps)
         a = engine_run(lmb, wl)
         assert 0.05 < np.mean(a["fo"]["flag"]) < 0.95
         for tag, b in (("record", engine_run(lmb, wl, record=True)), ("split", engine_run(lmb, wl, split=45))):
