@@ -98,7 +98,7 @@ k_milne(const KParams<R> kp, int64_t s0, int64_t s1)
     for (int64_t s = s0; s < s1; ++s) {
         const StepRec<R> sr = tab[s];
         milne_step<REC, R>(kp, sr, i, s, nk, x, xl, p);
-        if (!state_finite<R, 2, 2>(x, p)) {
+        if (!state_finite_all<R, 2, 2>(x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
         }

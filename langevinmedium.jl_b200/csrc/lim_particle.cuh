@@ -33,14 +33,33 @@ __device__ __forceinline__ void store_state(const KParams<R>& kp, int64_t i, con
     for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];
 }
 
+// Every component of the state is finite (the Milne kernel's test).
 template <typename R, int DIMS, int PDIM>
-__device__ __forceinline__ bool state_finite(const R (&x)[3], const double (&p)[3])
+__device__ __forceinline__ bool state_finite_all(const R (&x)[3], const double (&p)[3])
 {
     bool ok = true;
 #pragma unroll
     for (int d = 0; d < DIMS; ++d) ok &= (bool)isfinite(x[d]);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) ok &= (bool)isfinite(p[d]);
+    return ok;
+}
+
+// The Cartesian state after a step is finite.  In relativistic runs the position
+// decides: the step's streaming moves x by dt p / E with E = sqrt(m^2 + p.p) over every
+// momentum component, so a non-finite momentum makes x non-finite in the same step
+// (NaN or Inf in p gives NaN in p / E).  Galilean streaming divides by m and never sees
+// the components beyond DIMS, so there the momentum is checked as well.
+template <typename R, int DIMS, int PDIM>
+__device__ __forceinline__ bool state_finite(const KParams<R>& kp, const R (&x)[3], const double (&p)[3])
+{
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) ok &= (bool)isfinite(x[d]);
+    if (!kp.rel) {
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) ok &= (bool)isfinite(p[d]);
+    }
     return ok;
 }
 
@@ -92,7 +111,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             grid_rows(kp.med, kn, x[0], x[1], rows);
         }
         if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, frozen, lpos, lmom, ltau, lT, carry);
-        if (!state_finite<R, DIMS, PDIM>(x, p)) {
+        if (!state_finite<R, DIMS, PDIM>(kp, x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
         }

@@ -205,10 +205,17 @@ def test_empty_ensemble(lmb):
     eng.close()
 
 
-def test_nonfinite_state_is_reported(lmb):
-    """simulate_cpu.jl:293-303: NaN/Inf in the state stops the run with the step."""
-    wl = build_case("flow2d", "fp64", N=256, steps=10)
-    wl.p[0, 100] = np.nan
+@pytest.mark.parametrize("name,prec,comp,rel", [("flow2d", "fp64", 0, 1), ("flow2d", "fp32", 0, 1),
+                                               ("freezeout", "fp32", 2, 1), ("freezeout", "fp64", 2, 0)])
+def test_nonfinite_state_is_reported(lmb, name, prec, comp, rel):
+    """simulate_cpu.jl:293-303: NaN/Inf in the state stops the run with the step.  The
+    Cartesian kernels test the positions (a non-finite momentum reaches them through
+    E in the same step) and, in Galilean runs, the momenta too (p^z never reaches x
+    there)."""
+    wl = build_case(name, prec, N=256, steps=10)
+    wl.params["relativistic"] = rel
+    wl.params["stop_after_freezeout"] = 0
+    wl.p[comp, 100] = np.nan
     eng = lmb.capi.Engine(0)
     lmb.workloads.configure(eng, wl)
     with pytest.raises(lmb.capi.LimError, match="NaN/Inf at step 1") as ei:
