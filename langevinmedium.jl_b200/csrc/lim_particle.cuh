@@ -75,11 +75,18 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
     bool frozen = false;
     double ltau = 0.0, lT = 0.0;
-    double lpos[3] = { 0.0, 0.0, 0.0 }, lmom[3] = { 0.0, 0.0, 0.0 };
+    LatchPos<R> lpos;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { lpos.h[d] = R(0); lpos.l[d] = 0.0f; }
+    double lmom[3] = { 0.0, 0.0, 0.0 };
     if (FO) {
         frozen = kp.fo_flag[i] != 0.0; ltau = kp.l_tau[i]; lT = kp.l_T[i];
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) lpos[d] = kp.l_pos[d][i];
+        for (int d = 0; d < DIMS; ++d) {
+            const double v = kp.l_pos[d][i];   // FP32: split back into the pair it was stored from
+            lpos.h[d] = (R)v;
+            if (sizeof(R) == 4) lpos.l[d] = (float)(v - (double)lpos.h[d]);
+        }
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
     }
@@ -120,7 +127,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     if (FO) {
         kp.l_tau[i] = ltau; kp.l_T[i] = lT;
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos[d];
+        for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos.at(d);
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom[d];
     }

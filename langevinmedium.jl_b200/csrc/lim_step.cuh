@@ -888,6 +888,21 @@ __device__ __forceinline__ float temperature_screen(const KParams<R>& kp, const 
     return (float)temperature_at<R, MED, DIMS>(kp, sr, x, r);
 }
 
+// The latch's last-above position: in FP64 runs the position itself; in FP32 runs the
+// FP32 pair (x, x_lo) it was recorded from, summed in FP64 only where the position is
+// used (the same sum the record would have taken, so the same bits), which spares the
+// conversions on every step the particle stays above.
+template <typename R>
+struct LatchPos {
+    R h[3];
+    float l[3];
+    __device__ __forceinline__ double at(int d) const
+    {
+        if constexpr (sizeof(R) == 8) return h[d];
+        else return (double)h[d] + (double)l[d];
+    }
+};
+
 // Freeze-out latch after streaming (kernels_gpu.jl:588-635), evaluated in FP64.
 // FP32 path: the FP64 temperature is evaluated only when an FP32 screen puts T
 // within kScreen of Tfo; a last-above step recorded from the screen alone keeps
@@ -895,7 +910,7 @@ __device__ __forceinline__ float temperature_screen(const KParams<R>& kp, const 
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
                                                 const R (&x)[3], const float (&xl)[3], const double (&p)[3],
-                                                bool& frozen, double (&lpos)[3], double (&lmom)[3],
+                                                bool& frozen, LatchPos<R>& lpos, double (&lmom)[3],
                                                 double& ltau, double& lT, GridRows<R>* carry = nullptr)
 {
     constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
@@ -923,7 +938,10 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         }
         if (Ts >= (float)Tfo + kScreen) {            // clearly above: remember the step only
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
+            for (int d = 0; d < DIMS; ++d) {
+                if constexpr (sizeof(R) == 8) lpos.h[d] = xd[d];
+                else { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
+            }
 #pragma unroll
             for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
             ltau = sr.t;
@@ -933,13 +951,14 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
         if (T < Tfo && lT < 0.0) {
             const StepRec<R> pr = step_rec_at_time<R, MED>(kp, ltau);
-            lT = temperature_fp64<R, MED, DIMS>(kp, pr, lpos);
+            const double lp[3] = { lpos.at(0), lpos.at(1), lpos.at(2) };
+            lT = temperature_fp64<R, MED, DIMS>(kp, pr, lp);
         }
     }
     if (T < Tfo) {
         double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos[d] + frac * (xd[d] - lpos[d]);
+        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom[d] + frac * (p[d] - lmom[d]);
         kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
@@ -947,7 +966,10 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         frozen = true;
     } else {
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) lpos[d] = xd[d];
+        for (int d = 0; d < DIMS; ++d) {
+            if constexpr (sizeof(R) == 8) lpos.h[d] = xd[d];
+            else { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
+        }
 #pragma unroll
         for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
         ltau = sr.t;
