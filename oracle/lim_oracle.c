@@ -164,23 +164,17 @@ static double eval_spline(double T, double Tmin, double invdT, const double* val
     return (1.0 - t) * y0 + t * y1;
 }
 
-/* kernels_gpu.jl:88-117 — bilinear lookup of the Jüttner inverse CDF.  The u-cell is
- * located from the nearer end of the u grid: with mag = min(u, 1-u) (exact for u in
- * (0,1)), position mag (nU-1) counted from u = 0 or from u = 1.  In exact arithmetic
- * this is u (nU-1); it keeps the steep cells near u = 1 as finely resolved as those
- * near 0. */
+/* kernels_gpu.jl:88-117 — bilinear lookup of the Jüttner inverse CDF, in the
+ * reference's arithmetic: the fractional u-index fu = clamp(u, 0, 1) (nU - 1) computed
+ * directly, its floor capped to [0, nU-2]. */
 static double invcdf_lookup(const orc_medium* md, double u, double T)
 {
     int64_t nU = md->nU, nT = md->nT;
     double uu = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
-    const int up = uu > 0.5;
-    double mag = up ? 1.0 - uu : uu;
-    double fm = mag * (double)(nU - 1);
-    double k = floor(fm);
-    double fr = fm - k;
-    int64_t iu = up ? nU - 2 - (int64_t)k : (int64_t)k;
+    double fu = uu * (double)(nU - 1);
+    int64_t iu = (int64_t)floor(fu);
     iu = iu < 0 ? 0 : (iu > nU - 2 ? nU - 2 : iu);
-    double tu = up ? 1.0 - fr : fr;
+    double tu = fu - (double)iu;
     double fT = (T - md->ic_Tmin) * md->ic_invdT;
     int64_t jT = (int64_t)floor(fT);
     jT = jT < 0 ? 0 : (jT > nT - 2 ? nT - 2 : jT);
@@ -820,6 +814,9 @@ int64_t orc_run(const orc_params* P, const orc_medium* md, double* x, double* p,
                 if (fo && P->freezeout_capture) freezeout_latch(P, md, xs, ps, s * P->dt + P->t0, &fo[i]);
             }
             if (bad == INT64_MAX && nonfinite(P, xs, ps)) bad = s;
+            /* stop_after_freezeout: a latched particle is not advanced any further (its
+             * outputs are the latch's), as the engine's live-list runs do */
+            if (fo && P->freezeout_capture && P->stop_after_freezeout && fo[i].flag != 0.0) break;
             if (save_every > 0 && (s % save_every) == 0 && hist_x && hist_p) {
                 int64_t slot = s / save_every - first_slot;
                 for (int64_t d = 0; d < P->dims; ++d) hist_x[(slot * n + i) * P->dims + d] = xs[d];
