@@ -4,7 +4,9 @@ Restates the parts of LangevInMedium.jl's ``src/utils.jl`` that sit between the
 user's initial state and the time loop: the momentum-dimension contract
 ``check_momentum_dims`` (:561-573), the thermal p_z completion
 ``sample_pz_conditional_juttner`` / ``append_thermal_pz`` (:499-551), and the radial
-reduction of the drivers (simulate_cpu.jl:102-136).  Randomness comes from a numpy
+reduction of the drivers (simulate_cpu.jl:102-136), and the momentum-only initial state
+of the static-temperature path ``sample_initial_particles_at_origin_no_position!``
+(:419-465).  Randomness comes from a numpy
 Generator (the reference uses Julia's global RNG; draws are distributionally, not
 bitwise, equivalent).
 """
@@ -130,3 +132,27 @@ def _rt_interp_host(xgrid, tgrid, values, xi, yi) -> float:
     c0 = v[i, j] * (1 - xd) + v[i + 1, j] * xd
     c1 = v[i, j + 1] * (1 - xd) + v[i + 1, j + 1] * xd
     return float(c0 * (1 - yd) + c1 * yd)
+
+
+def sample_initial_particles_at_origin_no_position(initial_condition, p0, dimensions: int, N_particles: int,
+                                                   rng: np.random.Generator) -> np.ndarray:
+    """utils.jl:419-465 — the momenta (dimensions, N) of the static-temperature path:
+    "delta": |p| = p0 in a random direction (a normalised Gaussian vector); "bimodal":
+    |p| from an equal mixture of Normal(1, 0.2) and Normal(2, 0.2) truncated to
+    [0.1, 5], in a random direction; anything else is the reference's error."""
+    N, d = int(N_particles), int(dimensions)
+    if initial_condition == "delta":
+        dirs = rng.standard_normal((d, N))
+        return p0 * (dirs / np.sqrt(np.sum(dirs ** 2, axis=0)))
+    if initial_condition == "bimodal":
+        mu = np.where(rng.random(N) < 0.5, 1.0, 2.0)
+        mags = np.empty(N)
+        todo = np.arange(N)
+        while todo.size:                      # truncation to [pmin, pmax] by rejection
+            draw = rng.normal(mu[todo], 0.2)
+            ok = (draw >= 0.1) & (draw <= 5.0)
+            mags[todo[ok]] = draw[ok]
+            todo = todo[~ok]
+        dirs = rng.standard_normal((d, N))
+        return mags * (dirs / np.linalg.norm(dirs, axis=0))
+    raise ValueError(f"Unknown initial condition: {initial_condition}")

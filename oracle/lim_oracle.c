@@ -37,7 +37,7 @@
 enum { C_LANGEVIN = 0, C_RTA = 1, C_LANGEVIN_RTA = 2, C_FLUID = 3 };
 enum { M_RT = 0, M_BJORKEN = 1, M_GRID = 2 };
 enum { TAG_MOM = 1, TAG_RTA = 2, TAG_DIFF = 4, TAG_SAMPLE_XY = 5, TAG_SAMPLE_P = 6,
-       TAG_SAMPLE_PZ = 7 };
+       TAG_SAMPLE_PZ = 7, TAG_REJECT = 8 };
 
 typedef struct orc_params {
     double dt, t0, m, DsT, Tfo, psi2, obs_pt_cut, obs_pt_width;
@@ -282,6 +282,9 @@ double orc_norm_inv(double p) { return norm_inv(p); }
 typedef struct noise_src {
     const double* rec;      /* recorded buffer or NULL (Philox) */
     int64_t rec_first, rec_steps, n;
+    /* decision record or NULL: dec[(step - rec_first) * n + i] gets bit 0 when the
+     * particle collides (RTA) and bit 1 when it latches at freeze-out in that step */
+    uint8_t* dec;
 } noise_src;
 
 static inline double rec_at(const noise_src* ns, int64_t i, int64_t step, int slot)
@@ -550,6 +553,7 @@ static void rta_collide(const orc_params* P, const orc_medium* md, const noise_s
     int collide = uc < Pcol || Pcol >= 1.0;
     if (P->rta_replay && ns->rec) collide = rec_at(ns, i, step, 4) != 0.0;
     if (!collide) return;
+    if (ns->dec) ns->dec[(step - ns->rec_first) * ns->n + i] |= 1u;
     double us, g[3];
     draw_rta_sample(P, ns, i, step, &us, g);
     double pstar = invcdf_lookup(md, us, T);
@@ -794,9 +798,9 @@ void orc_initial_lab_boost(const orc_params* P, const orc_medium* md, double* x,
  */
 int64_t orc_run(const orc_params* P, const orc_medium* md, double* x, double* p, int64_t n,
                 int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,
-                double* hist_x, double* hist_p, fo_state* fo, const double* rec, int threads)
+                double* hist_x, double* hist_p, fo_state* fo, const double* rec, int threads, uint8_t* dec)
 {
-    noise_src ns = { rec, first_step, nsteps, n };
+    noise_src ns = { rec, first_step, nsteps, n, dec };
     int64_t first_bad = INT64_MAX;
 #ifdef _OPENMP
     int nth = threads > 0 ? threads : omp_get_max_threads();
@@ -808,15 +812,19 @@ int64_t orc_run(const orc_params* P, const orc_medium* md, double* x, double* p,
         for (int64_t d = 0; d < P->pdim; ++d) ps[d] = p[i * P->pdim + d];
         int64_t bad = INT64_MAX;
         for (int64_t s = first_step; s < first_step + nsteps; ++s) {
-            if (P->coords == 1) milne_step(P, md, &ns, i, s, xs, ps);
-            else {
-                cart_step(P, md, &ns, i, s, xs, ps);
-                if (fo && P->freezeout_capture) freezeout_latch(P, md, xs, ps, s * P->dt + P->t0, &fo[i]);
-            }
-            if (bad == INT64_MAX && nonfinite(P, xs, ps)) bad = s;
             /* stop_after_freezeout: a latched particle is not advanced any further (its
              * outputs are the latch's), as the engine's live-list runs do */
             if (fo && P->freezeout_capture && P->stop_after_freezeout && fo[i].flag != 0.0) break;
+            if (P->coords == 1) milne_step(P, md, &ns, i, s, xs, ps);
+            else {
+                cart_step(P, md, &ns, i, s, xs, ps);
+                if (fo && P->freezeout_capture) {
+                    const double was = fo[i].flag;
+                    freezeout_latch(P, md, xs, ps, s * P->dt + P->t0, &fo[i]);
+                    if (dec && was == 0.0 && fo[i].flag != 0.0) dec[(s - first_step) * n + i] |= 2u;
+                }
+            }
+            if (bad == INT64_MAX && nonfinite(P, xs, ps)) bad = s;
             if (save_every > 0 && (s % save_every) == 0 && hist_x && hist_p) {
                 int64_t slot = s / save_every - first_slot;
                 for (int64_t d = 0; d < P->dims; ++d) hist_x[(slot * n + i) * P->dims + d] = xs[d];
@@ -828,6 +836,98 @@ int64_t orc_run(const orc_params* P, const orc_medium* md, double* x, double* p,
         if (bad < first_bad) first_bad = bad;
     }
     return first_bad == INT64_MAX ? -1 : first_bad;
+}
+
+/* kernels_cpu.jl:442-458 (_draw_juttner_pstar_lib): the CPU RTA's Juttner magnitude
+ * sampler for P(p) ~ p^(d-1) exp(-(E - m)/T), by rejection under the flat envelope
+ * 1.3 x the exact peak on [0, pmax), pmax = 16 sqrt(m T) + 16 T, at most 1e5 tries (then
+ * the peak momentum).  Its two uniforms per try come from Philox, counter
+ * (pid, try, TAG_REJECT), instead of Julia's global rand(); in the reference only the
+ * GPU form (the inverse-CDF table) takes injected uniforms.  Used to compare the two
+ * samplers' distributions.  tries[k]: the tries the k-th draw took. */
+static double juttner_pstar_rejection(const orc_params* P, double m, double T, int64_t d, int64_t pid,
+                                      int64_t* tries)
+{
+    *tries = 0;
+    if (T <= 0.0) return 0.0;
+    const double a = (double)(d - 1);
+    const double E_peak = (a * T + sqrt(a * a * T * T + 4.0 * m * m)) / 2.0;
+    const double p_peak = sqrt(jl_max(E_peak * E_peak - m * m, 1e-12));
+    const double gpeak = pow(p_peak, a) * exp(-(E_peak - m) / T);     /* 0^0 = 1, as in Julia */
+    const double wmax = 1.3 * jl_max(gpeak, 1e-300);
+    const double pmax = 16.0 * sqrt(m * T) + 16.0 * T;
+    for (int64_t t = 0; t < 100000; ++t) {
+        double u[4];
+        uniforms4(P, pid, t, TAG_REJECT, u);
+        const double p = pmax * u[0];
+        const double E = sqrt(m * m + p * p);
+        const double w = pow(p, a) * exp(-(E - m) / T);
+        *tries = t + 1;
+        if (u[1] * wmax <= w) return p;
+    }
+    return p_peak;
+}
+
+void orc_juttner_rejection(const orc_params* P, double m, double T, int64_t d, int64_t first_pid, int64_t n,
+                           double* out, int64_t* tries)
+{
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t k = 0; k < n; ++k) out[k] = juttner_pstar_rejection(P, m, T, d, first_pid + k, &tries[k]);
+}
+
+/* simulate_cpu.jl:325-404 with the legacy force kernels_cpu.jl:359-404 and the update
+ * :406-417: the static-temperature momentum-only path.  kappa = 2.5 T^3,
+ * eta_D = kappa / (2 T m), kL = kT = sqrt(kappa); per component det = -eta_D p dt and
+ * sto = sum_j ((kL - kT) u_d u_j + kT delta_dj) xi_j, which is kT xi_d because
+ * kL - kT = 0; p += det + sqrt(dt) sto.  The momentum normals are the step's (TAG_MOM).
+ * |p| after every step s with s % save_every == 0 goes to hist[(s / save_every -
+ * first_slot) n + i] for slots in [0, nslots). */
+void orc_run_static(const orc_params* P, double T, double* p, int64_t n, int64_t first_step, int64_t nsteps,
+                    int64_t save_every, int64_t first_slot, int64_t nslots, double* hist, int threads)
+{
+    noise_src ns = { NULL, 0, 0, 0, NULL };
+    const double kappa = 2.5 * (T * T * T);
+    const double etaD = kappa / (2.0 * T * P->m);
+    const double kL = sqrt(kappa), kT = sqrt(kappa);
+    const double sq = sqrt(P->dt);
+    const int64_t pd = P->pdim;
+#ifdef _OPENMP
+    int nth = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nth)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        double ps[3] = { 0, 0, 0 };
+        for (int64_t d = 0; d < pd; ++d) ps[d] = p[i * pd + d];
+        for (int64_t s = first_step; s < first_step + nsteps; ++s) {
+            double xi[3], uc;
+            draw_step(P, &ns, i, s, 1, xi, &uc);
+            double pm = 0.0;
+            for (int64_t d = 0; d < pd; ++d) pm += ps[d] * ps[d];
+            pm = sqrt(pm);
+            double u[3];                       /* p_units: the projector term multiplies them by 0 */
+            for (int64_t d = 0; d < pd; ++d) u[d] = pm < 2.220446049250313e-16 ? 0.0 : ps[d] / pm;
+            double det[3], sto[3];
+            for (int64_t d = 0; d < pd; ++d) {
+                det[d] = -etaD * ps[d] * P->dt;
+                double acc = 0.0;
+                for (int64_t j = 0; j < pd; ++j)
+                    acc += (kL - kT) * u[d] * u[j] * xi[j] + kT * (d == j ? 1.0 : 0.0) * xi[j];
+                sto[d] = acc;
+            }
+            for (int64_t d = 0; d < pd; ++d) ps[d] += det[d] + sq * sto[d];
+            if (save_every > 0 && hist && s % save_every == 0) {
+                const int64_t slot = s / save_every - first_slot;
+                if (slot >= 0 && slot < nslots) {
+                    double p2 = 0.0;
+                    for (int64_t d = 0; d < pd; ++d) p2 += ps[d] * ps[d];
+                    hist[slot * n + i] = sqrt(p2);
+                }
+            }
+        }
+        for (int64_t d = 0; d < pd; ++d) p[i * pd + d] = ps[d];
+    }
 }
 
 /* Helpers exported for tests. */
@@ -843,7 +943,7 @@ void orc_uniforms4(const orc_params* P, int64_t pid, int64_t step, int tag, doub
  * as if the particle collided (slots 4..7 are drawn regardless). */
 void orc_step_variates(const orc_params* P, int64_t i, int64_t step, int kick, double out[11])
 {
-    noise_src ns = { NULL, 0, 0, 0 };
+    noise_src ns = { NULL, 0, 0, 0, NULL };
     double xi[3], uc, us, g[3], d[3];
     for (int k = 0; k < 11; ++k) out[k] = 0.0;
     draw_step(P, &ns, i, step, kick, xi, &uc);

@@ -64,7 +64,7 @@ def lib() -> C.CDLL:
         build()
         L = C.CDLL(str(LIB))
         L.orc_run.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcMedium), _DP, _DP, C.c_int64, C.c_int64, C.c_int64,
-                              C.c_int64, C.c_int64, _DP, _DP, _DP, _DP, C.c_int]
+                              C.c_int64, C.c_int64, _DP, _DP, _DP, _DP, C.c_int, C.POINTER(C.c_uint8)]
         L.orc_run.restype = C.c_int64
         L.orc_initial_lab_boost.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcMedium), _DP, _DP, C.c_int64]
         L.orc_initial_lab_boost.restype = None
@@ -89,6 +89,12 @@ def lib() -> C.CDLL:
         L.orc_sample_milne.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, _DP, _DP, _DP, _DP,
                                        _DP, C.c_int64, C.c_int64, _DP, _DP]
         L.orc_sample_milne.restype = C.c_int64
+        L.orc_juttner_rejection.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, C.c_int64,
+                                            C.c_int64, _DP, C.POINTER(C.c_int64)]
+        L.orc_juttner_rejection.restype = None
+        L.orc_run_static.argtypes = [C.POINTER(OrcParams), C.c_double, _DP, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                                     C.c_int64, C.c_int64, _DP, C.c_int]
+        L.orc_run_static.restype = None
         L.orc_sample_pz.argtypes = [C.POINTER(OrcParams), C.c_double, C.c_double, C.c_int64, _DP]
         L.orc_sample_pz.restype = None
         assert L.orc_sizeof_params() == C.sizeof(OrcParams)
@@ -194,8 +200,12 @@ def initial_lab_boost(P: OrcParams, md: Medium, x, p):
 
 
 def run(P: OrcParams, md: Medium, x, p, first_step, nsteps, *, save_every=0, first_slot=0, nslots=0,
-        fo=None, rec=None, threads=0):
-    """Run the restatement.  Returns dict(x, p, first_bad, hist_x, hist_p, fo)."""
+        fo=None, rec=None, threads=0, decisions=False):
+    """Run the restatement.  Returns dict(x, p, first_bad, hist_x, hist_p, fo), and with
+    decisions=True "dec": uint8 (nsteps, N), bit 0 = the particle collided (RTA) in
+    that step, bit 1 = it latched at freeze-out in that step.  fo: an initial latch
+    state (N * FO_FIELDS doubles, per particle pos[3], mom[3], tau, flag, lpos[3],
+    lmom[3], ltau, lT), zeros when None."""
     n = np.asarray(x).shape[-1]
     xb, pb = to_flat(x, P.dims), to_flat(p, P.pdim)
     hx = hp = None
@@ -209,9 +219,13 @@ def run(P: OrcParams, md: Medium, x, p, first_step, nsteps, *, save_every=0, fir
     if rec is not None:
         recb = np.ascontiguousarray(rec, dtype=np.float64).reshape(-1)
         assert recb.size == nsteps * NOISE_SLOTS * n
+    dec = np.zeros((nsteps, n), dtype=np.uint8) if decisions else None
     bad = lib().orc_run(C.byref(P), C.byref(md.s), _d(xb), _d(pb), n, first_step, nsteps, save_every, first_slot,
-                        _d(hx), _d(hp), _d(fob), _d(recb), int(threads))
+                        _d(hx), _d(hp), _d(fob), _d(recb), int(threads),
+                        None if dec is None else dec.ctypes.data_as(C.POINTER(C.c_uint8)))
     out = dict(x=from_flat(xb, P.dims, n), p=from_flat(pb, P.pdim, n), first_bad=int(bad), fo=fob)
+    if dec is not None:
+        out["dec"] = dec
     if hx is not None:
         out["hist_x"] = [from_flat(hx[k * n * P.dims:(k + 1) * n * P.dims], P.dims, n) for k in range(nslots)]
         out["hist_p"] = [from_flat(hp[k * n * P.pdim:(k + 1) * n * P.pdim], P.pdim, n) for k in range(nslots)]
@@ -221,6 +235,10 @@ def run(P: OrcParams, md: Medium, x, p, first_step, nsteps, *, save_every=0, fir
         out["fo_mom"] = f[:, 3:3 + P.pdim].T.copy()
         out["fo_tau"] = f[:, 6].copy()
         out["fo_flag"] = f[:, 7].copy()
+        out["fo_lpos"] = f[:, 8:8 + P.dims].T.copy()
+        out["fo_lmom"] = f[:, 11:11 + P.pdim].T.copy()
+        out["fo_ltau"] = f[:, 14].copy()
+        out["fo_lT"] = f[:, 15].copy()
     return out
 
 
@@ -281,3 +299,30 @@ def sample_milne(P: OrcParams, x_lo, x_hi, T_c, ur_c, mu_c, r_T, T_r, n):
     failed = lib().orc_sample_milne(C.byref(P), float(x_lo), float(x_hi), a[0].size, _d(a[0]), _d(a[1]), _d(a[2]),
                                     _d(a[3]), _d(a[4]), a[3].size, int(n), _d(xb), _d(pb))
     return from_flat(xb[:2 * n], 2, n), from_flat(pb[:2 * n], 2, n), int(failed)
+
+
+def juttner_rejection(P: OrcParams, m: float, T: float, d: int, n: int, first_pid: int = 0):
+    """n draws of the CPU RTA's rejection sampler (kernels_cpu.jl:442-458) with Philox
+    uniforms; returns (p*, tries per draw)."""
+    out = np.zeros(n)
+    tries = np.zeros(n, dtype=np.int64)
+    lib().orc_juttner_rejection(C.byref(P), float(m), float(T), int(d), int(first_pid), int(n), _d(out),
+                                tries.ctypes.data_as(C.POINTER(C.c_int64)))
+    return out, tries
+
+
+def invcdf_lookup(md: "Medium", u: float, T: float) -> float:
+    """The inverse-CDF table lookup of the GPU RTA (kernels_gpu.jl:88-117)."""
+    return float(lib().orc_invcdf_lookup(C.byref(md.s), float(u), float(T)))
+
+
+def run_static(P: OrcParams, T: float, p, first_step: int, nsteps: int, *, save_every=0, first_slot=0, nslots=0,
+               threads=0):
+    """The static-temperature momentum-only path (simulate_cpu.jl:325-404); returns
+    (p (pdim, N), |p| history (nslots, N))."""
+    n = np.asarray(p).shape[-1]
+    pb = to_flat(p, P.pdim)
+    hist = np.zeros((max(nslots, 0), n))
+    lib().orc_run_static(C.byref(P), float(T), _d(pb), n, int(first_step), int(nsteps), int(save_every),
+                         int(first_slot), int(nslots), _d(hist) if nslots > 0 else None, int(threads))
+    return from_flat(pb, P.pdim, n), hist
