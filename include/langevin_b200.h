@@ -20,7 +20,7 @@
  *   - src/simulate.jl:117-141 (CPU_GCBackend, Milne (tau, r) coordinates)
  *   - src/simulate_cpu.jl:215-316 / src/simulate_gpu.jl:283-392 (the step loop)
  *   - src/simulate_cpu_general_coords.jl:83-126 (the Milne step loop)
- * A Julia caller reaches these through ccall.
+ * A Julia caller reaches these through ccall with the signatures below.
  */
 #ifndef LANGEVIN_B200_H
 #define LANGEVIN_B200_H
@@ -290,13 +290,16 @@ int lim_observables(lim_ctx* ctx, int from_freezeout, double* out);
  * (memory comes from their own pool, e.g. CUDA.jl's, or the call runs where
  * allocation is not allowed).  p_dev: (pdim, n) column-major doubles on `device`;
  * x_dev: (dims, n) or NULL; out_dev: LIM_OBS_NUM doubles on the device receiving
- * the SUMS (out[LIM_OBS_COUNT] = n; divide for means).  Enqueued on `stream`
+ * the SUMS (out[LIM_OBS_COUNT] = n; divide for means).  pt_width <= 0 means 1e-3
+ * (as in lim_observables).  Enqueued on `stream`
  * (NULL = default stream); read out_dev after the stream reaches the call.
  * Limits and sharing: n <= 16,777,216; the per-block partial sums live in one
  * fixed 96 KiB device array of the library, held by every GPU that loads it until
  * the process exits, shared by all calls: calls that overlap on the GPU (e.g. on
  * two streams at once) race.  The first call on a device looks up that array's
- * device address; make it before any stream capture.  Errors: lim_last_error(NULL). */
+ * device address; make it before any stream capture.  A CUDA error left pending by
+ * earlier work on the calling thread is reported (LIM_ERR_CUDA) before anything is
+ * launched.  Errors: lim_last_error(NULL). */
 int lim_observables_noalloc(int device, const double* p_dev, int64_t pdim, const double* x_dev,
                             int64_t dims, int64_t n, double m, double pt_cut, double pt_width,
                             double* out_dev, void* stream);

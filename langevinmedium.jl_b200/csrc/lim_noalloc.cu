@@ -11,6 +11,7 @@
 #include <mutex>
 #include "../../include/langevin_b200.h"
 #include "lim_internal.h"
+#include "lim_obs.cuh"
 
 namespace {
 
@@ -21,7 +22,8 @@ constexpr long long kNAMaxParticles = (long long)kNABlocks * kNAThreads * kNAPer
 constexpr int kNAObs = lim::kObsNum;
 
 // One FP64 partial row per block.  Every call overwrites the rows it uses and reads
-// only those, so nothing needs clearing; concurrent calls on different streams share it.
+// only those, so nothing needs clearing.  All calls share it: calls that overlap on the
+// GPU (for example on two streams) race on it, so the caller serialises them.
 static __device__ __align__(256) double g_obs_scratch[kNABlocks * kNAObs];
 
 constexpr int kMaxDevices = 64;
@@ -38,42 +40,12 @@ k_obs_noalloc_partials(const double* __restrict__ p, int pdim, const double* __r
     for (int k = 0; k < kNAObs; ++k) v[k] = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        double q[3] = { 0.0, 0.0, 0.0 };
+        double q[3] = { 0.0, 0.0, 0.0 }, y[3] = { 0.0, 0.0, 0.0 };
         for (int d = 0; d < pdim; ++d) q[d] = p[i * pdim + d];
-        const double px = q[0], py = pdim >= 2 ? q[1] : 0.0;
-        const double pt2 = px * px + py * py, pt = sqrt(pt2);
-        double p2 = 0.0;
-        for (int d = 0; d < pdim; ++d) p2 += q[d] * q[d];
-        const double E = sqrt(m * m + p2), w = m / E;
-        v[0] += 1.0;
-        v[1] += pt;
-        v[2] += pt2 > 0.0 ? (px * px - py * py) / pt2 : 0.0;
-        v[3] += pt > cut ? 1.0 : 0.0;
-        v[4] += 1.0 / (1.0 + exp(-(pt - cut) / width));
-        v[5] += p2;
-        v[6] += E;
-        v[7] += w * p2;
-        v[8] += px;
-        v[9] += w * px;
-        v[10] += pdim == 3 ? q[2] * q[2] : 0.0;
-        double x2 = 0.0;
-        for (int d = 0; d < dims; ++d) { const double xd = x[i * dims + d]; x2 += xd * xd; }
-        v[11] += x2;
+        for (int d = 0; d < dims; ++d) y[d] = x[i * dims + d];
+        lim::obs_add_terms(q, y, pdim, dims, m, cut, width, v);
     }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < kNAObs; ++k) {
-        double a = v[k];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
-        if (lane == 0) sh[warp][k] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < kNAObs) {
-        double a = 0.0;
-        for (int w = 0; w < kNAThreads / 32; ++w) a += sh[w][threadIdx.x];
-        partials[(long long)blockIdx.x * kNAObs + threadIdx.x] = a;
-    }
+    lim::obs_block_sum(v, sh, partials + (long long)blockIdx.x * kNAObs);
 }
 
 __global__ void k_obs_noalloc_total(const double* __restrict__ partials, int nblocks, double* __restrict__ out)
@@ -133,6 +105,15 @@ extern "C" int lim_observables_noalloc(int device, const double* p_dev, int64_t 
     long long blocks = (n + kNAThreads - 1) / kNAThreads;
     blocks = blocks < 1 ? 1 : (blocks > kNABlocks ? kNABlocks : blocks);
     cudaStream_t st = (cudaStream_t)stream;
+    // an error left pending by earlier work on this thread is reported as such, so that
+    // the status after the launches below belongs to this call
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        if (prev != device) cudaSetDevice(prev);
+        snprintf(buf, sizeof buf, "lim_observables_noalloc: a CUDA error was pending before the call: %s",
+                 cudaGetErrorString(e));
+        return noalloc_fail(LIM_ERR_CUDA, buf);
+    }
     k_obs_noalloc_partials<<<(unsigned)blocks, kNAThreads, 0, st>>>(p_dev, (int)pdim, x_dev, x_dev ? (int)dims : 0,
                                                                      (long long)n, m, pt_cut,
                                                                      pt_width > 0 ? pt_width : 1e-3, scratch);

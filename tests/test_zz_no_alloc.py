@@ -29,13 +29,16 @@ def context_sums(capi, x, p, m, cut, width):
 
 
 def noalloc_sums(capi, x, p, m, cut, width):
+    """x = None: no positions (x_dev = NULL, dims = 0)."""
     lib = capi.load_library()
-    dims, pdim, n = x.shape[0], p.shape[0], p.shape[1]
-    xd = torch.from_numpy(capi.julia_layout(x, dims).copy()).cuda()
+    pdim, n = p.shape[0], p.shape[1]
+    dims = 0 if x is None else x.shape[0]
+    xd = None if x is None else torch.from_numpy(capi.julia_layout(x, dims).copy()).cuda()
     pd = torch.from_numpy(capi.julia_layout(p, pdim).copy()).cuda()
     out = torch.full((capi.LIM_OBS_NUM,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    rc = lib.lim_observables_noalloc(0, C.c_void_p(pd.data_ptr()), pdim, C.c_void_p(xd.data_ptr()), dims, n,
+    rc = lib.lim_observables_noalloc(0, C.c_void_p(pd.data_ptr()), pdim,
+                                     None if xd is None else C.c_void_p(xd.data_ptr()), dims, n,
                                      m, cut, width, C.c_void_p(out.data_ptr()), C.c_void_p(stream))
     assert rc == capi.LIM_OK, lib.lim_last_error(None)
     torch.cuda.synchronize()
@@ -68,3 +71,26 @@ def test_noalloc_rejects_sizes_beyond_the_scratch_limit(lmb):
     rc = lib.lim_observables_noalloc(0, C.c_void_p(out.data_ptr()), 4, None, 0, 10, 1.5, 5.0, 0.1,
                                      C.c_void_p(out.data_ptr()), None)
     assert rc == capi.LIM_ERR_ARG
+
+
+def test_noalloc_without_positions_and_with_zero_width(lmb):
+    """x_dev = NULL (dims 0) leaves the |x|^2 sum at zero and the momentum sums as the
+    context path gives them; pt_width <= 0 stands for 1e-3 in both entry points."""
+    capi = lmb.capi
+    rng = np.random.default_rng(7)
+    n, m, cut = 40_000, 4.75, 1.0
+    p = rng.normal(0.0, 1.2, (3, n))
+    x = rng.normal(0.0, 2.0, (2, n))
+    ref = context_sums(capi, x, p, m, cut, 0.2)
+    got = noalloc_sums(capi, None, p, m, cut, 0.2)
+    assert got[11] == 0.0
+    np.testing.assert_allclose(got[:11], ref[:11], rtol=1e-12, atol=1e-9)
+    ref0 = context_sums(capi, x, p, m, cut, 0.0)
+    got0 = noalloc_sums(capi, x, p, m, cut, 0.0)
+    np.testing.assert_allclose(got0, ref0, rtol=1e-12, atol=1e-9)
+
+
+def test_noalloc_empty_ensemble_gives_zeros(lmb):
+    capi = lmb.capi
+    got = noalloc_sums(capi, None, np.zeros((3, 0)), 1.5, 5.0, 0.1)
+    assert np.array_equal(got, np.zeros(capi.LIM_OBS_NUM))
