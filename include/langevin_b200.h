@@ -237,6 +237,19 @@ int lim_run(lim_ctx* ctx, int64_t first_step, int64_t nsteps,
             int64_t save_every, int64_t first_slot,
             double* hist_x, double* hist_p);
 
+/* The static-temperature momentum-only path: simulate_ensemble_bulk(::CPUBackend,
+ * T::Float64; ...) (src/simulate.jl:89-109 -> src/simulate_cpu.jl:325-404) with its
+ * legacy force (src/kernels_cpu.jl:359-404): kappa = 2.5 T^3, eta_D = kappa / (2 T m),
+ * Euler drag -eta_D p dt and the kick sqrt(dt) sqrt(kappa) xi on the uploaded momenta
+ * (pdim rows; the positions and any medium are not used), with the context's dt, m,
+ * precision, seed and particle_offset.  |p| after every step s with s % save_every == 0
+ * goes to hist_pmag[(s / save_every - first_slot) * n + i] for slots in [0, nslots)
+ * (the host array is copied in first, so slots not written keep their values: the
+ * reference's slot 0, the initial |p|, is the caller's).  As in the reference driver,
+ * no non-finite check. */
+int lim_run_static_T(lim_ctx* ctx, double T, int64_t first_step, int64_t nsteps, int64_t save_every,
+                     int64_t first_slot, int64_t nslots, double* hist_pmag);
+
 /* ---- snapshots reduced on the device ---------------------------------------------
  * In place of the FP64 snapshot history (simulate_cpu.jl:319-322: pdim x N x nslots
  * momenta and positions, 38 GB for 1e7 particles and 95 saves), each snapshot is

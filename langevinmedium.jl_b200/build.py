@@ -27,7 +27,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
 ]
 SOURCES = ["lim_kernels.cu", "lim_capi.cu", "lim_noalloc.cu", "lim_batch.cu", "lim_batch_capi.cu", "lim_sample.cu", "lim_reduce.cu", "lim_tables.cu",
-           "lim_adjoint.cu", "lim_adjoint_capi.cu"]
+           "lim_adjoint.cu", "lim_adjoint_capi.cu", "lim_static.cu"]
 
 
 def nvcc_path() -> str:

@@ -133,6 +133,8 @@ _SIGS = {
     "lim_state_save": ([C.c_void_p], C.c_int),
     "lim_state_restore": ([C.c_void_p], C.c_int),
     "lim_run": ([C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _DP, _DP], C.c_int),
+    "lim_run_static_T": ([C.c_void_p, C.c_double, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64, _DP],
+                         C.c_int),
     "lim_status": ([C.c_void_p, _I64P], C.c_int),
     "lim_download_freezeout": ([C.c_void_p, _DP, _DP, _DP, _DP], C.c_int),
     "lim_observables": ([C.c_void_p, C.c_int, _DP], C.c_int),
@@ -417,6 +419,16 @@ class Engine:
         self._check(self.lib.lim_run(self.ctx, int(first_step), int(nsteps), int(save_every), int(first_slot),
                                      _dptr(hist_x), _dptr(hist_p)))
 
+    def run_static_T(self, T: float, first_step: int, nsteps: int, save_every: int = 0, first_slot: int = 0,
+                     hist_pmag: np.ndarray | None = None):
+        """The static-temperature momentum-only path (lim_run_static_T); hist_pmag: a
+        (nslots, N) array of |p| snapshots, slot s / save_every - first_slot."""
+        nslots = 0 if hist_pmag is None else int(hist_pmag.shape[0])
+        if hist_pmag is not None and (hist_pmag.dtype != np.float64 or not hist_pmag.flags.c_contiguous):
+            raise ValueError("hist_pmag must be a C-contiguous float64 array of shape (nslots, N)")
+        self._check(self.lib.lim_run_static_T(self.ctx, float(T), int(first_step), int(nsteps), int(save_every),
+                                              int(first_slot), nslots, _dptr(hist_pmag)))
+
     def reduce_state(self, spec: LimReduceSpec) -> dict:
         """The current state reduced on the device (lim_reduce_state): one slot."""
         out = np.zeros(max(int(self.lib.lim_reduce_stride(C.byref(spec))), 1))   # an invalid spec fails below
@@ -442,6 +454,12 @@ class Engine:
         self._check(self.lib.lim_download_freezeout(self.ctx, _dptr(fp), _dptr(fm), _dptr(ft), _dptr(ff)))
         return dict(pos=from_julia_layout(fp[:n * dims], dims, n), mom=from_julia_layout(fm[:n * pdim], pdim, n),
                     tau=ft[:n].copy(), flag=ff[:n].copy())
+
+    def download_freezeout_flat(self, fo_pos, fo_mom, fo_tau, fo_flag):
+        """Freeze-out outputs into caller buffers in the Julia layout (e.g. page-locked
+        host memory): fo_pos (dims, n), fo_mom (pdim, n), fo_tau (n), fo_flag (n)."""
+        self._check(self.lib.lim_download_freezeout(self.ctx, _dptr(fo_pos), _dptr(fo_mom), _dptr(fo_tau),
+                                                    _dptr(fo_flag)))
 
     def observables(self, from_freezeout: bool = False) -> dict:
         out = np.zeros(LIM_OBS_NUM)

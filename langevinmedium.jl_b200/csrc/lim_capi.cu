@@ -156,6 +156,10 @@ int ensure_device_medium(lim_ctx* c)
         for (size_t k = 0; k < s.size(); ++k) s[k] = (R)c->icdf[k];
         if ((rc = upload(c, c->d_icdf, s.data(), s.size()))) return rc;
     }
+    if (sizeof(R) == 4) {                 // FP64 copies for the FP32 path's near-threshold RTA decisions
+        if (!c->spl[1].empty() && (rc = upload(c, c->d_rta64, c->spl[1].data(), c->spl[1].size()))) return rc;
+        if (c->med_kind == MED_RT && (rc = upload(c, c->d_T64, c->T.data(), c->T.size()))) return rc;
+    }
     c->dev_prec = prec;
     c->dev_dirty = false;
     return LIM_OK;
@@ -207,6 +211,13 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
     kp.rta_mode = c->d_rta_bits.p ? c->rta_mode : 0;
     kp.rta_first = c->rta_first;
     kp.rta_steps = c->rta_steps;
+    if (sizeof(R) == 4) {
+        kp.rta64 = c->spl[1].empty() ? nullptr : (const double*)c->d_rta64.p;
+        kp.rta_Tmin64 = c->spl_Tmin[1];
+        kp.rta_invdT64 = c->spl_invdT[1];
+        kp.n_rta64 = (int)c->spl[1].size();
+        kp.T64 = c->med_kind == MED_RT ? (const double*)c->d_T64.p : nullptr;
+    }
     kp.icdf = (const R*)c->d_icdf.p; kp.nU = (int)c->nU; kp.nT = (int)c->nT;
     kp.ic_Tmin = (R)c->ic_Tmin; kp.ic_invdT = (R)c->ic_invdT;
     MediumDev<R>& md = kp.med;
@@ -685,7 +696,8 @@ int lim_destroy(lim_ctx* c)
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
                       &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
-                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p };
+                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p, &c->d_pmag_hist,
+                      &c->d_rta64, &c->d_T64 };
     for (DevBuf* b : all) dev_free(*b);
     for (int d = 0; d < 3; ++d) {
         dev_free(c->d_x[d]); dev_free(c->d_xlo[d]); dev_free(c->d_p[d]);
@@ -718,7 +730,8 @@ int lim_device_bytes(const lim_ctx* c, int64_t* bytes)
                       &c->d_live[0], &c->d_live[1], &c->d_live_n, &c->d_rta_bits,
                       &c->d_adj_ckpt, &c->d_adj_tape, &c->d_adj_table, &c->d_adj_part, &c->d_adj_out,
                       &c->d_adj_lam, &c->d_adj_gacc, &c->d_adj_slope, &c->d_adj_icdt, &c->d_sample,
-                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p };
+                      &c->d_red_obs, &c->d_red_hist, &c->d_stage2_x, &c->d_stage2_p, &c->d_pmag_hist,
+                      &c->d_rta64, &c->d_T64 };
     int64_t t = 0;
     for (const DevBuf* b : all) t += (int64_t)b->bytes;
     for (int d = 0; d < 3; ++d)
@@ -1379,6 +1392,58 @@ int lim_reduce_state(lim_ctx* c, const lim_reduce_spec* spec, double* out)
         if ((rc = build_kparams<double>(c, kp)) || (rc = reduce_snapshot<double>(c, kp, red, 0))) return rc;
     }
     return reduce_download(c, red, out);
+}
+
+int lim_run_static_T(lim_ctx* c, double T, int64_t first_step, int64_t nsteps, int64_t save_every,
+                     int64_t first_slot, int64_t nslots, double* hist_pmag)
+{
+    if (!c) return LIM_ERR_ARG;
+    if (!c->have_params) return fail(c, LIM_ERR_STATE, "lim_set_params must be called before running");
+    if (!c->have_state) return fail(c, LIM_ERR_STATE, "no particle state uploaded (lim_upload_state)");
+    if (c->state_prec != (int)c->P.precision)
+        return fail(c, LIM_ERR_STATE, "state was uploaded in another precision; upload it again");
+    if (c->P.coords != LIM_COORDS_CARTESIAN)
+        return fail(c, LIM_ERR_UNSUPPORTED, "lim_run_static_T: the static-temperature path is Cartesian");
+    if (nsteps < 0) return fail(c, LIM_ERR_ARG, "lim_run_static_T: negative step count");
+    if (first_step < 0 || first_step + nsteps > (int64_t)UINT32_MAX)
+        return fail(c, LIM_ERR_ARG, "lim_run_static_T: steps must lie in [0, 2^32)");
+    if (save_every < 0 || nslots < 0) return fail(c, LIM_ERR_ARG, "lim_run_static_T: negative save_every or nslots");
+    const bool saving = save_every > 0 && nslots > 0 && hist_pmag;
+    const double hist_bytes = saving ? (double)nslots * (double)c->n * sizeof(double) : 0.0;
+    if (hist_bytes > 16.0e9) return fail(c, LIM_ERR_ARG, "lim_run_static_T: history of %.3g bytes is too large", hist_bytes);
+    cudaSetDevice(c->device);
+    StaticRun sr{};
+    for (int d = 0; d < 3; ++d) sr.p[d] = d < c->pdim ? (double*)c->d_p[d].p : nullptr;
+    sr.n = c->n;
+    sr.pid_offset = c->P.particle_offset;
+    sr.T = T;
+    sr.m = c->P.m;
+    sr.dt = c->P.dt;
+    {
+        uint32_t k0 = (uint32_t)(uint64_t)c->P.seed, k1 = (uint32_t)((uint64_t)c->P.seed >> 32);
+        for (int r = 0; r < 10; ++r) { sr.rk[r] = make_uint2(k0, k1); k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    }
+    sr.save_every = saving ? save_every : 0;
+    sr.first_slot = first_slot;
+    sr.nslots = saving ? nslots : 0;
+    if (saving && c->n > 0) {
+        int rc = dev_alloc(c, c->d_pmag_hist, (size_t)hist_bytes);
+        if (rc) return rc;
+        LIM_CUDA(c, cudaMemcpyAsync(c->d_pmag_hist.p, hist_pmag, (size_t)hist_bytes, cudaMemcpyHostToDevice, c->stream));
+        sr.hist = (double*)c->d_pmag_hist.p;
+    }
+    LIM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    LIM_CUDA(c, c->state_prec == LIM_FP32 ? launch_static_T<float>(sr, c->pdim, first_step, first_step + nsteps, c->stream)
+                                          : launch_static_T<double>(sr, c->pdim, first_step, first_step + nsteps, c->stream));
+    LIM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    if (saving && c->n > 0)
+        LIM_CUDA(c, cudaMemcpyAsync(hist_pmag, c->d_pmag_hist.p, (size_t)hist_bytes, cudaMemcpyDeviceToHost, c->stream));
+    LIM_CUDA(c, cudaStreamSynchronize(c->stream));
+    float ms = 0.0f;
+    LIM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->last_ms = ms;
+    c->last_launches = (c->n > 0 && nsteps > 0) ? 1 : 0;
+    return LIM_OK;
 }
 
 int lim_run_reduced(lim_ctx* c, int64_t first_step, int64_t nsteps, int64_t save_every, int64_t first_slot,

@@ -106,6 +106,11 @@ struct alignas(16) KParams {
     const R* drag_da; const R* drag_db;
     const float4* adj_drag; const R* icdf_dT;
     float* tape; int64_t tape_first;
+    // FP32 runs: the RTA spline and the (r, t) temperature table in FP64, for collision
+    // decisions that fall within FP32 rounding of the collision probability (decided
+    // again in FP64, as the FP64 path decides them); NULL in FP64 runs
+    const double* rta64; double rta_Tmin64, rta_invdT64; int n_rta64;
+    const double* T64;
 };
 
 // ---------------------------------------------------------------------------
@@ -268,9 +273,35 @@ __device__ __forceinline__ float u_centered(uint32_t w, float)
     return fmaf(__int2float_rn((int32_t)(w ^ 0x80000000u)), 0x1p-31f, 0x1p-32f);
 }
 
+// sin(pi a) and cos(pi a) for a in [-1, 1] in FP32: a = r + q/2 with q = rint(2a) and
+// |r| <= 1/4 (exact), the Taylor series of sin(pi r) (through r^9) and cos(pi r)
+// (through r^10) in r^2 by Horner's rule (truncation below 3e-9), then the quadrant
+// q selects and signs them.  Absolute error about 1.5e-7 (the arguments' and results'
+// FP32 rounding), against 2^-21.4 = 3.6e-7 of the hardware sine/cosine.
+__device__ __forceinline__ void sincospi_f32(float a, float& s, float& c)
+{
+    const float q = rintf(2.0f * a);
+    const float r = fmaf(-0.5f, q, a);
+    const float z = r * r;
+    float ps = fmaf(z, 0.08214588661112823f, -0.5992645293207921f);
+    ps = fmaf(ps, z, 2.5501640398773455f);
+    ps = fmaf(ps, z, -5.16771278004997f);
+    ps = fmaf(ps, z, 3.141592653589793f);
+    float pc = fmaf(z, -0.02580689139001406f, 0.2353306303588932f);
+    pc = fmaf(pc, z, -1.3352627688545895f);
+    pc = fmaf(pc, z, 4.0587121264167685f);
+    pc = fmaf(pc, z, -4.934802200544679f);
+    const float sn = r * ps, cs = fmaf(pc, z, 1.0f);
+    const int qi = (int)q;
+    const bool swap = (qi & 1) != 0;
+    s = swap ? cs : sn;
+    c = swap ? sn : cs;
+    if ((qi + 4) & 2) s = -s;      // quadrants q = 2, -1, -2
+    if ((qi + 5) & 2) c = -c;      // quadrants q = 1, 2, -2
+}
+
 // Box–Muller with the angle in (-pi, pi): (rad cos(pi(2u1-1)), rad sin(pi(2u1-1))),
-// rad = sqrt(-2 ln u0).  FP32 uses the hardware sine/cosine, accurate to 2^-21.4
-// absolute on [-pi, pi].
+// rad = sqrt(-2 ln u0); FP32 takes the sine and cosine from sincospi_f32.
 __device__ __forceinline__ void box_muller(uint32_t w0, uint32_t w1, double& z0, double& z1)
 {
     const double rad = sqrt(neg2_log_u(w0, 0.0));
@@ -282,7 +313,7 @@ __device__ __forceinline__ void box_muller(uint32_t w0, uint32_t w1, float& z0, 
 {
     const float rad = sqrtf(neg2_log_u(w0, 0.0f));
     float s, c;
-    __sincosf(3.14159265358979f * u_centered(w1, 0.0f), &s, &c);
+    sincospi_f32(u_centered(w1, 0.0f), s, c);
     z0 = rad * c; z1 = rad * s;
 }
 

@@ -57,6 +57,8 @@ struct lim_ctx {
     lim::DevBuf d_rta_bits;               // recorded / replayed RTA decisions
     lim::DevBuf d_sample;                 // sampling tables (lim_sample_fonll)
     lim::DevBuf d_red_obs, d_red_hist;    // snapshot reductions (lim_run_reduced)
+    lim::DevBuf d_pmag_hist;              // |p| history of lim_run_static_T
+    lim::DevBuf d_rta64, d_T64;           // FP32 runs: FP64 RTA spline and (r, t) T table
     int rta_mode = 0;
     int64_t rta_first = 0, rta_steps = 0;
     lim::DevBuf d_adj_ckpt, d_adj_tape, d_adj_table, d_adj_part, d_adj_out;   // lim_adjoint

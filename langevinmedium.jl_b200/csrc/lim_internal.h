@@ -26,6 +26,19 @@ cudaError_t launch_compact_live(const double* flag, const int* in, const unsigne
 template <typename R>
 size_t step_record_bytes();
 
+// The static-temperature momentum-only run (simulate_cpu.jl:325-404): the FP64 momenta
+// p[d][i], the run constants and the |p| history hist[(s / save_every - first_slot) n + i].
+struct StaticRun {
+    double* p[3];
+    int64_t n, pid_offset;
+    double T, m, dt;
+    uint2 rk[10];
+    double* hist;
+    int64_t save_every, first_slot, nslots;
+};
+template <typename R>
+cudaError_t launch_static_T(const StaticRun& sr, int pdim, int64_t s0, int64_t s1, cudaStream_t st);
+
 // Step-0 lab boost (simulate_cpu.jl:160-163).
 template <typename R>
 cudaError_t launch_lab_boost(const KParams<R>& kp, int block, cudaStream_t st);

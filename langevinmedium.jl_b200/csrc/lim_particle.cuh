@@ -73,14 +73,17 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     double p[3];
     float xl[3];
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    bool frozen = false;
+    bool frozen = false, have_last = false;
     double ltau = 0.0, lT = 0.0;
     LatchPos<R> lpos;
+    LatchMom<R> lmom;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { lpos.h[d] = R(0); lpos.l[d] = 0.0f; }
-    double lmom[3] = { 0.0, 0.0, 0.0 };
+    for (int d = 0; d < 3; ++d) { lpos.h[d] = R(0); lpos.l[d] = 0.0f; lmom.m[d] = 0; }
     if (FO) {
+        // the latch record of the previous launch; l_T = 0 until a particle has one (in FP32
+        // runs the record holds -1 there and the temperature is re-evaluated at the crossing)
         frozen = kp.fo_flag[i] != 0.0; ltau = kp.l_tau[i]; lT = kp.l_T[i];
+        have_last = lT != 0.0;
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) {
             const double v = kp.l_pos[d][i];   // FP32: split back into the pair it was stored from
@@ -88,7 +91,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             if (sizeof(R) == 4) lpos.l[d] = (float)(v - (double)lpos.h[d]);
         }
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) lmom[d] = kp.l_mom[d][i];
+        for (int d = 0; d < PDIM; ++d) lmom.m[d] = kp.l_mom[d][i];
     }
     const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
@@ -110,14 +113,16 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             *t = make_float4((float)x[0], (float)x[1], (float)p[0], (float)p[1]);
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];
         }
-        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, carry);
+        float pf[3];
+        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
         if constexpr (kCarry) {
             // the next step's time row: from the table inside the launch, computed past it
             double w;
             const int kn = s + 1 < s1 ? tab[s + 1].kt : grid_time_cell(kp.med, step_time(kp, s + 1), w);
             grid_rows(kp.med, kn, x[0], x[1], rows);
         }
-        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, frozen, lpos, lmom, ltau, lT, carry);
+        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last,
+                                                    carry);
         if (!state_finite<R, DIMS, PDIM>(kp, x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
@@ -125,11 +130,12 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     }
     store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
     if (FO) {
-        kp.l_tau[i] = ltau; kp.l_T[i] = lT;
+        kp.l_tau[i] = ltau;
+        kp.l_T[i] = sizeof(R) == 4 ? (have_last ? -1.0 : 0.0) : lT;
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos.at(d);
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom[d];
+        for (int d = 0; d < PDIM; ++d) kp.l_mom[d][i] = lmom.at(d);
     }
 }
 

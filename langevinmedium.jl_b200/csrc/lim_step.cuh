@@ -15,6 +15,7 @@
 //                      (u1,u2) -> directions g0, g1, g2 = Phi^-1(u3)   [slots 4-7]
 //   group DIFF position-diffusion normals                              [slots 8-10]
 #pragma once
+#include <type_traits>
 #include "lim_common.cuh"
 
 namespace lim {
@@ -339,6 +340,26 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     return L;
 }
 
+// 1/sqrt(s) and sqrt(s) for s > 0 in the FP32 kernels' FP64 frame change: the FP32
+// hardware estimate refined by one Newton step in FP64 (relative error below 1e-13, far
+// inside FP32 resolution; the FP64 kernels keep the correctly rounded forms for FP64
+// parity).  Each is one FP32 estimate and three FP64 operations in place of a
+// correctly rounded FP64 square root and division.
+__device__ __forceinline__ double rsqrt_f32_newton(double s)
+{
+    const double r = (double)rsqrtf((float)s);
+    const double h = 0.5 * fma(-s * r, r, 1.0);
+    return fma(r, h, r);
+}
+__device__ __forceinline__ double sqrt_f32_newton(double s)
+{
+    const float sf = (float)s;
+    if (!(sf > 0.0f && sf < 3.0e38f)) return sqrt(s);       // 0, FP32 overflow, NaN: the plain form
+    const float r0 = rsqrtf(sf);
+    const double e0 = (double)(sf * r0);
+    return fma(0.5 * (double)r0, fma(-e0, e0, s), e0);
+}
+
 // kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  The frame
 // change is evaluated in FP64 in both precisions: with the momentum held in FP64,
 // p_par - v E does not lose the LRF momentum to cancellation at large gamma, and no
@@ -351,6 +372,7 @@ __device__ __forceinline__ double boost_gamma(const Local<R>& L)
 {
     const double vmax = 0.9999999999995;   // sqrt(1 - 1e-12)
     const double v = jclamp((double)L.v, -vmax, vmax);
+    if constexpr (sizeof(R) == 4) return rsqrt_f32_newton(1.0 - v * v + 1e-10);
     return 1.0 / sqrt(1.0 - v * v + 1e-10);
 }
 
@@ -374,11 +396,12 @@ __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, d
     }
     const double vmax = 0.9999999999995;   // sqrt(1 - 1e-12)
     v = jclamp(v, -vmax, vmax);
-    const double gam = gamp > 0.0 ? gamp : 1.0 / sqrt(1.0 - v * v + 1e-10);
+    double gam = gamp;
+    if (!(gam > 0.0)) gam = sizeof(R) == 4 ? rsqrt_f32_newton(1.0 - v * v + 1e-10) : 1.0 / sqrt(1.0 - v * v + 1e-10);
     double p2 = 0.0;
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) p2 += p[d] * p[d];
-    double E = sqrt(p2 + m * m);
+    const double E = sizeof(R) == 4 ? sqrt_f32_newton(p2 + m * m) : sqrt(p2 + m * m);
     double vE = to_lab ? v * E : -(v * E);
     if (DIMS == 1) { p[0] = gam * (p[0] + vE); return; }
     double px = p[0], py = p[1];
@@ -526,17 +549,46 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, uint32_t w, R T
     return c0 * (R(1) - tT) + c1 * tT;
 }
 
+template <typename R, int MED, int DIMS>
+__device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const StepRec<R>& sr, const double (&xd)[3]);
+
+// The collision decision of the FP64 path, for an FP32 step whose collision uniform falls
+// within 1e-5 (relative) of its FP32 collision probability: the medium temperature at the
+// pre-step position, the RTA time and the probability in FP64 (kernels_gpu.jl:675-688),
+// compared with the uniform's exact value.  This gives the FP64 path's decision up to
+// the FP64 rounding of the temperature (the FP32 decision alone would flip wherever the
+// two probabilities straddle the uniform: a few per 1e9 particle-steps).
+template <typename R, int MED, int DIMS>
+__device__ __forceinline__ bool rta_decide_fp64(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
+                                                const float (&xl)[3], uint32_t wc)
+{
+    const double xd[3] = { (double)x[0] + (double)xl[0], (double)x[1] + (double)xl[1], (double)x[2] + (double)xl[2] };
+    const double T = jmax0(temperature_fp64<R, MED, DIMS>(kp, sr, xd));
+    double tn = 0.0;
+    if ((double)kp.DsT > 0.0 && T > 0.0)
+        tn = spline_at(kp.rta64, spline_index(T, kp.rta_Tmin64, kp.rta_invdT64, kp.n_rta64));
+    const double Pcol = (tn > 0.0 && isfinite(tn)) ? jclamp(kp.dt / tn, 0.0, 1.0) : 1.0;
+    return u_exact(wc) < Pcol || Pcol >= 1.0;
+}
+
 // kernels_gpu.jl:653-704: with probability Pcol = clamp(dt/tau, 0, 1) re-draw |p*|
 // from the Jüttner inverse CDF and an isotropic direction.  The collision
 // uniform u_collide comes with the step's momentum variates; the sample and the
 // direction are drawn only when the particle collides.
 // tn: the RTA relaxation time (0 when DsT <= 0 or T <= 0), kernels_gpu.jl:675-679.
-template <int REC, typename R, int DIMS, int PDIM>
+// wc: the collision word (uc = u_value<R>(wc)); sr, x, xl: the step record and the
+// pre-step position (for the FP32 path's near-threshold FP64 decision).
+template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, const NoiseKey& nk,
-                                            R T, R tn, R uc, double (&p)[3])
+                                            R T, R tn, uint32_t wc, const StepRec<R>& sr, const R (&x)[3],
+                                            const float (&xl)[3], double (&p)[3])
 {
+    const R uc = u_value<R>(wc);
     R Pcol = (tn > R(0) && isfinite(tn)) ? jclamp(kp.dtR / tn, R(0), R(1)) : R(1);
     bool collide = uc < Pcol || Pcol >= R(1);
+    if constexpr (sizeof(R) == 4) {
+        if (kp.rta64 && fabsf(uc - Pcol) <= 1e-5f * Pcol) collide = rta_decide_fp64<R, MED, DIMS>(kp, sr, x, xl, wc);
+    }
     if (kp.rta_mode && s >= kp.rta_first && s < kp.rta_first + kp.rta_steps) {
         uint32_t* w = kp.rta_bits + ((s - kp.rta_first) >> 5) * kp.n + i;
         const uint32_t bit = 1u << ((s - kp.rta_first) & 31);
@@ -703,10 +755,11 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
 }
 
 // One Cartesian step (simulate_cpu.jl:215-290).
+// pf_out (optional): the lab momentum after the step, rounded to FP32.
 template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3],
-                                          GridRows<R>* carry = nullptr)
+                                          GridRows<R>* carry = nullptr, float* pf_out = nullptr)
 {
     // the grid medium's tape rows 0, 2, 3 (pre-step momentum, medium and gradient); row 1
     // (the normals and v^x) follows the kick
@@ -765,11 +818,15 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
             R tn = R(0);
             if (kp.DsT > R(0) && T > R(0))
                 tn = spline_at(kp.rta, kp.spl_shared ? sd : spline_index(T, kp.rta_Tmin, kp.rta_invdT, kp.n_rta));
-            rta_collide<REC, R, DIMS, PDIM>(kp, i, s, nk, T, tn, u_value<R>(wc), p);
+            rta_collide<REC, R, MED, DIMS, PDIM>(kp, i, s, nk, T, tn, wc, sr, x, xl, p);
         }
         if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true, gam);
     }
     stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
+    if (pf_out) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pf_out[d] = (float)p[d];
+    }
 }
 
 // Temperature at the particle in FP64 arithmetic (FP64 weights over the stored
@@ -795,8 +852,14 @@ __device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const S
         double x0 = g[i], x1 = g[i + 1], dx = x1 - x0;
         double w = fabs(dx) < kEps ? 0.0 : (rq - x0) / dx;
         const int j = sr.kt;
-        double v00 = (double)md.TV[i + nr * j].x, v10 = (double)md.TV[i + 1 + nr * j].x;
-        double v01 = (double)md.TV[i + nr * (j + 1)].x, v11 = (double)md.TV[i + 1 + nr * (j + 1)].x;
+        double v00, v10, v01, v11;
+        if (kp.T64) {                    // FP32 runs: the FP64 table the FP64 path interpolates
+            v00 = kp.T64[i + nr * j]; v10 = kp.T64[i + 1 + nr * j];
+            v01 = kp.T64[i + nr * (j + 1)]; v11 = kp.T64[i + 1 + nr * (j + 1)];
+        } else {
+            v00 = (double)md.TV[i + nr * j].x; v10 = (double)md.TV[i + 1 + nr * j].x;
+            v01 = (double)md.TV[i + nr * (j + 1)].x; v11 = (double)md.TV[i + 1 + nr * (j + 1)].x;
+        }
         double c0 = v00 * (1.0 - w) + v10 * w, c1 = v01 * (1.0 - w) + v11 * w;
         T = c0 * (1.0 - sr.wtd) + c1 * sr.wtd;
     } else {
@@ -903,24 +966,38 @@ struct LatchPos {
     }
 };
 
+// The latch's last-above momentum: FP64 in FP64 runs; in FP32 runs the step's lab
+// momentum rounded to FP32 (the latch interpolates it with the current FP64 momentum,
+// so its rounding reaches the latched momentum at 6e-8 relative).
+template <typename R>
+struct LatchMom {
+    typename std::conditional<sizeof(R) == 8, double, float>::type m[3];
+    __device__ __forceinline__ double at(int d) const { return (double)m[d]; }
+};
+
 // Freeze-out latch after streaming (kernels_gpu.jl:588-635), evaluated in FP64.
-// FP32 path: the FP64 temperature is evaluated only when an FP32 screen puts T
-// within kScreen of Tfo; a last-above step recorded from the screen alone keeps
-// lT = -1, and its FP64 temperature is re-evaluated from (lpos, ltau) when needed.
+// FP64 path: the temperature at the particle in FP64 every step; the last-above
+// temperature lT is kept.  FP32 path: the FP64 temperature is evaluated only when an
+// FP32 screen puts T within kScreen of Tfo; the last-above temperature is not kept but
+// re-evaluated in FP64 from the recorded position and time at the crossing (the same
+// evaluation as at that step, so the same bits); have_last tells whether there is a
+// last-above record at all (a particle already below Tfo at its first step latches with
+// frac = 1, as with lT = 0 in the reference).  pf: the step's lab momentum in FP32.
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
                                                 const R (&x)[3], const float (&xl)[3], const double (&p)[3],
-                                                bool& frozen, LatchPos<R>& lpos, double (&lmom)[3],
-                                                double& ltau, double& lT, GridRows<R>* carry = nullptr)
+                                                const float (&pf)[3], bool& frozen, LatchPos<R>& lpos,
+                                                LatchMom<R>& lmom, double& ltau, double& lT, bool& have_last,
+                                                GridRows<R>* carry = nullptr)
 {
     constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
     if (frozen) return;
-    double xd[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (sizeof(R) == 4 ? (double)xl[d] : 0.0);
     const double Tfo = (double)kp.Tfo;
     double T;
-    if (sizeof(R) == 8) {
+    if constexpr (sizeof(R) == 8) {
+        double xd[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xd[d] = (double)x[d];
         R r;
         if (DIMS == 1) r = fabs(x[0]);
         else { R r2 = R(0);
@@ -928,6 +1005,24 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
             for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
             r = sqrt(r2); }
         T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
+        if (T < Tfo) {
+            const double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
+#pragma unroll
+            for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom.at(d) + frac * (p[d] - lmom.at(d));
+            kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
+            kp.fo_flag[i] = 1.0;
+            frozen = true;
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIMS; ++d) lpos.h[d] = xd[d];
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) lmom.m[d] = p[d];
+            ltau = sr.t;
+            lT = T;
+            have_last = true;
+        }
     } else {
         float Ts;
         if (MED == MED_GRID && carry) {      // the next step's rows at the new position
@@ -936,44 +1031,36 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         } else {
             Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
         }
-        if (Ts >= (float)Tfo + kScreen) {            // clearly above: remember the step only
+        if (!(Ts >= (float)Tfo + kScreen)) {
+            double xd[3];
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) {
-                if constexpr (sizeof(R) == 8) lpos.h[d] = xd[d];
-                else { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
+            for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (double)xl[d];
+            T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
+            if (T < Tfo) {
+                double lTv = 0.0;
+                if (have_last) {
+                    const StepRec<R> pr = step_rec_at_time<R, MED>(kp, ltau);
+                    const double lp[3] = { lpos.at(0), lpos.at(1), lpos.at(2) };
+                    lTv = temperature_fp64<R, MED, DIMS>(kp, pr, lp);
+                }
+                const double frac = (kp.fo_interp && lTv > Tfo && lTv > T) ? (lTv - Tfo) / (lTv - T) : 1.0;
+#pragma unroll
+                for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
+#pragma unroll
+                for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom.at(d) + frac * (p[d] - lmom.at(d));
+                kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
+                kp.fo_flag[i] = 1.0;
+                frozen = true;
+                return;
             }
-#pragma unroll
-            for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
-            ltau = sr.t;
-            lT = -1.0;
-            return;
         }
-        T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
-        if (T < Tfo && lT < 0.0) {
-            const StepRec<R> pr = step_rec_at_time<R, MED>(kp, ltau);
-            const double lp[3] = { lpos.at(0), lpos.at(1), lpos.at(2) };
-            lT = temperature_fp64<R, MED, DIMS>(kp, pr, lp);
-        }
-    }
-    if (T < Tfo) {
-        double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
+        // above Tfo: remember this step (position pair, FP32 momentum, time)
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
+        for (int d = 0; d < DIMS; ++d) { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom[d] + frac * (p[d] - lmom[d]);
-        kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
-        kp.fo_flag[i] = 1.0;
-        frozen = true;
-    } else {
-#pragma unroll
-        for (int d = 0; d < DIMS; ++d) {
-            if constexpr (sizeof(R) == 8) lpos.h[d] = xd[d];
-            else { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
-        }
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) lmom[d] = p[d];
+        for (int d = 0; d < PDIM; ++d) lmom.m[d] = pf[d];
         ltau = sr.t;
-        lT = T;
+        have_last = true;
     }
 }
 

@@ -205,6 +205,36 @@ function LM.Simulate.simulate_ensemble_bulk(
     return time_points, [hp[:, :, i] for i in 1:num_saves+1], [hx[:, :, i] for i in 1:num_saves+1]
 end
 
+# ---- simulate_ensemble_bulk(::B200Backend, T::Float64; ...) — mirrors simulate.jl:89-109 ----------
+# The static-temperature momentum-only path (simulate_cpu.jl:325-404, legacy force
+# kernels_cpu.jl:359-404) on the device; the initial momenta come from the reference's
+# own sample_initial_particles_at_origin_no_position! (utils.jl:419-465), the |p|
+# history starts with their magnitudes.
+function LM.Simulate.simulate_ensemble_bulk(
+    backend::B200Backend, T::Float64;
+    N_particles::Int = 10_000, Δt::Float64 = 0.001, initial_time::Float64 = 0.0, final_time::Float64 = 1.0,
+    save_interval::Float64 = 0.1, m::Float64 = 1.0, p0 = 1.0, DsT = 0.2, initial_condition = "delta",
+    dimensions::Int = 3, seed::Integer = 0x4C494D00, precision::Symbol = :fp64, device::Integer = 0)
+
+    steps = floor(Int, (final_time - initial_time) / Δt)
+    save_every = round(Int, save_interval / Δt)
+    num_saves = div(steps, save_every)
+    momenta = LM.Utils.sample_initial_particles_at_origin_no_position!(initial_condition, p0, dimensions, N_particles)
+    N = size(momenta, 2)
+    c = create(device)
+    set_params(c, LimParams(Δt, initial_time, m, Float64(DsT), 0.0, 0.0, 5.0, 0.1, dimensions, dimensions, 0,
+        LIM_COLL[:langevin], 1, 0, 0, 0, 0, 0, 1, precision == :fp32 ? 1 : 0, Int64(seed), 0, 0, 0))
+    check(c.ptr, ccall((:lim_upload_state, libpath[]), Cint, (Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Float64}, Int64, Int64),
+        c.ptr, zeros(dimensions, N), dimensions, Matrix{Float64}(momenta), dimensions, N))
+    hist = zeros(N, num_saves + 1)                  # column k: the |p| snapshot of slot k-1
+    hist[:, 1] .= vec(sqrt.(sum(momenta .^ 2, dims = 1)))
+    check(c.ptr, ccall((:lim_run_static_T, libpath[]), Cint,
+        (Ptr{Cvoid}, Float64, Int64, Int64, Int64, Int64, Int64, Ptr{Float64}),
+        c.ptr, T, 1, steps, save_every, 0, num_saves + 1, hist))
+    time_points = range(initial_time, final_time, length = num_saves + 1)
+    return time_points, [hist[:, k] for k in 1:num_saves+1]
+end
+
 # ---- simulate_ensemble_bulk(::B200_GCBackend, ...) — mirrors simulate.jl:117-141 ----------------
 # sample_initial_particles_milne! (utils.jl:350-400) runs on the device: the profiles are
 # evaluated at the 200 bin centers of (0, maximum(xgrid)), and T(r) for the momentum

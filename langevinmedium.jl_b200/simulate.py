@@ -63,13 +63,50 @@ def _time_points(t0: float, tf: float, n: int) -> np.ndarray:
 
 
 def simulate_ensemble_bulk(backend, *args, **kwargs):
-    """Dispatch on the backend marker (simulate.jl:21, :117; simulate_gpu_wrapper.jl:15, :74)."""
+    """Dispatch on the backend marker and the first positional argument (simulate.jl:21,
+    :89, :117; simulate_gpu_wrapper.jl:15, :74): a real temperature selects the
+    static-temperature momentum-only path."""
     if isinstance(backend, B200Backend):
+        if len(args) == 1 and isinstance(args[0], (int, float, np.floating, np.integer)):
+            return _simulate_static_T(float(args[0]), **kwargs)
         return _simulate_cartesian(*args, **kwargs)
     if isinstance(backend, B200_GCBackend):
         return _simulate_milne(*args, **kwargs)
     raise TypeError(f"simulate_ensemble_bulk: no method for backend {type(backend).__name__} "
                     "(use B200Backend() or B200_GCBackend())")
+
+
+def _simulate_static_T(T: float, *, N_particles: int = 10_000, Δt: float = 0.001, initial_time: float = 0.0,
+                       final_time: float = 1.0, save_interval: float = 0.1, m: float = 1.0, p0=1.0, DsT=0.2,
+                       initial_condition="delta", dimensions: int = 3,
+                       # additive
+                       seed: int = DEFAULT_SEED, precision: str = "fp64", device: int = 0, stream=None,
+                       block_size: int = 0):
+    """simulate_ensemble_bulk(::CPUBackend, T::Float64; ...) (simulate.jl:89-109 ->
+    simulate_cpu.jl:325-404): momentum-only Langevin at a fixed temperature with the
+    legacy force kappa = 2.5 T^3 (kernels_cpu.jl:359-404).  Returns (time_points,
+    momenta_history) with one |p| vector per saved step (the initial one first).  DsT
+    is accepted and, as in the reference, not used."""
+    total_time = final_time - initial_time
+    steps = int(math.floor(total_time / Δt))
+    save_every = int(round(save_interval / Δt))
+    if save_every == 0:
+        raise ZeroDivisionError("save_interval/Δt rounds to 0 (DivideError in the reference)")
+    num_saves = steps // save_every
+    rng = np.random.default_rng(int(seed) & 0xFFFFFFFFFFFFFFFF)
+    from .utils import sample_initial_particles_at_origin_no_position
+    momenta = sample_initial_particles_at_origin_no_position(initial_condition, p0, dimensions, N_particles, rng)
+    N = momenta.shape[1]
+    hist = np.zeros((num_saves + 1, N))
+    hist[0] = np.sqrt(np.sum(momenta ** 2, axis=0))
+    eng = _engine(device, stream)
+    eng.set_params(dt=Δt, t0=initial_time, m=m, DsT=float(DsT), dims=int(dimensions), pdim=int(dimensions),
+                   precision=capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64, seed=int(seed),
+                   block_size=block_size)
+    eng.upload_state(np.zeros((int(dimensions), N)), momenta)
+    eng.run_static_T(T, 1, steps, save_every, 0, hist)
+    time_points = _time_points(initial_time, final_time, num_saves + 1)
+    return time_points, [hist[k].copy() for k in range(num_saves + 1)]
 
 
 def _simulate_cartesian(r_grid_Langevin, p_grid_Langevin, heavy_quark_density,

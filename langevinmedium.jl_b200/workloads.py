@@ -15,11 +15,12 @@ medium from the same description.
                 T0 = 0.45 GeV (σx 3.0, σy 2.4 fm) × (0.6/τ)^(1/3), radial flow
                 u^r = tanh(0.05 r (τ-0.6)) read as the flow velocity (the reference's
                 velocity fields are velocities), freeze-out latch at T < 0.155 GeV, Δt = 0.01.
-  adjoint_grid — the grid medium for pathwise gradients: 1e6 charm, 2000 steps, no
-                freeze-out, 2πT·D_s = a + b (T/0.155 - 1) and a temperature scale s.
+  adjoint_grid — the grid medium for pathwise gradients: 1e6 charm, 2000 steps of
+                Δt = 0.0047 (τ 0.6 → 10), no freeze-out, 2πT·D_s = a + b (T/0.155 - 1)
+                and a temperature scale s.
   batch       — 256 independent ensembles (counts log-uniform in [1e3, 1e6], charm or
-                bottom, 2πT·D_s ~ U[2,8], 500-2000 steps), half Bjorken, half 2+1D grids
-                with T0 ~ U[0.35,0.55] GeV and σy/σx ~ U[0.7,1.0].
+                bottom, 2πT·D_s ~ U[2,8], 500-2000 steps capped to τ ≤ 10), half Bjorken,
+                half 2+1D grids with T0 ~ U[0.35,0.55] GeV and σy/σx ~ U[0.7,1.0].
 """
 from __future__ import annotations
 
@@ -207,9 +208,10 @@ def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3,
           grid_shape=(201, 201, 100), offset0=0):
     """E independent ensembles for one batched launch: particle counts log-uniform in
     n_range, masses from {1.5, 4.75} GeV, 2πT·D_s uniform in [2, 8], step counts uniform
-    in steps_range; half use the Bjorken medium (analytic T(τ), Δτ = 0.005), half 2+1D
-    grids with T0 uniform in [0.35, 0.55] GeV and σy/σx uniform in [0.7, 1.0] (σx = 3 fm,
-    Δt = 0.01).  Langevin + RTA, no freeze-out.  Particle ids are consecutive across
+    in steps_range and capped to the medium's τ range 0.6 → 10 fm/c (1880 steps of the
+    Bjorken ensembles, 940 of the grid ones); half use the Bjorken medium (analytic T(τ),
+    Δτ = 0.005), half 2+1D grids with T0 uniform in [0.35, 0.55] GeV and σy/σx uniform in
+    [0.7, 1.0] (σx = 3 fm, Δt = 0.01).  Langevin + RTA, no freeze-out.  Particle ids are consecutive across
     ensembles (particle_offset), so every ensemble has its own noise."""
     rng = np.random.default_rng(rng_seed)
     nx, ny, nt = grid_shape
@@ -227,6 +229,7 @@ def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3,
         prec = capi.LIM_FP32 if precision == "fp32" else capi.LIM_FP64
         if kinds[e] == "bjorken":
             T0, tau0, dt = 0.40, 0.6, 0.005
+            steps = min(steps, int(math.floor((10.0 - tau0) / dt)))      # the medium's tau range, 0.6 -> 10
             med = dict(kind="bjorken", T0=T0, tau0=tau0, power=1.0 / 3.0, r_max=20.0)
             Tmin, Tmax = T0 * (tau0 / (tau0 + (steps + 2) * dt)) ** (1.0 / 3.0), T0
             x = rng.normal(0.0, 3.0, (2, n))
@@ -236,6 +239,7 @@ def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3,
             sx = 3.0
             sy = sx * float(rng.uniform(0.7, 1.0))
             tau0, dt = 0.6, 0.01
+            steps = min(steps, int(math.floor((10.0 - tau0) / dt)))      # the grid's tau range, 0.6 -> 10
             med = grid2p1_lazy(nx=nx, ny=ny, nt=nt, T0=T0, sx=sx, sy=sy)
             # the field's minimum: the grid corner at the last slice (grid2p1_fields)
             xm, ym = (nx - 1) / 2 * 0.1, (ny - 1) / 2 * 0.1
@@ -257,10 +261,12 @@ def batch(E=256, *, precision="fp32", seed=0x4C494D04, rng_seed=4, n_range=(1e3,
 
 
 def adjoint_grid(N=1_000_000, *, a=3.0, b=2.0, scale=1.0, steps=2000, m=1.5, precision="fp32",
-                 seed=0x4C494D03, rng_seed=5, dt=0.01, fields=None, eta_over_s=0.16, pt_cut=5.0, pt_width=0.1):
+                 seed=0x4C494D03, rng_seed=5, dt=0.0047, fields=None, eta_over_s=0.16, pt_cut=5.0, pt_width=0.1):
     """Differentiation workload: the 2+1D grid medium, charm, Langevin + RTA, no freeze-out,
     2πT·D_s = a + b (max(T, 0.155)/0.155 - 1), medium temperature scale s.  The drag
-    spline comes with its derivative tables in (a, b) for lim_adjoint."""
+    spline comes with its derivative tables in (a, b) for lim_adjoint.  dt = 0.0047 fm/c:
+    2000 steps span the grid's τ range 0.6 → 10 fm/c (with a longer step the run would
+    leave the grid's last time slice, where the medium is held constant)."""
     med = fields or grid2p1_fields()
     tau0 = med["tau0"]
     rng = np.random.default_rng(rng_seed)
