@@ -1,0 +1,57 @@
+"""The adjoint at the differentiation configuration's size: the full 201 x 201 x 100
+grid medium, 2000 steps of 0.0047 fm/c (tau 0.6 -> 10), checkpoints every 64 steps,
+on a 1e5-particle sample of charm quarks.  The gradient of <pT>, <cos 2 phi> and the
+smoothed fraction above 5 GeV with respect to (a, b, s) against central finite
+differences (h = 1e-3) of FP64 engine runs with common random numbers and the adjoint
+run's RTA decisions replayed.
+
+Gate, per entry, relative to max(|FD|, 1e-3 |obs|): within 1e-3 of FD(h) where the
+finite difference itself is settled (|FD(h) - FD(h/2)| below 1e-4 of the same scale);
+elsewhere within 1e-3 of the Richardson value 2 FD(h/2) - FD(h) plus twice the
+finite-difference spread (the tabulated medium and transport tables are piecewise
+linear, so a difference quotient straddling a node carries a share of the slope jump).
+Both figures are printed."""
+import numpy as np
+import pytest
+
+from test_gpu_adjoint import central_differences, compare, observables
+
+pytestmark = pytest.mark.gpu
+
+THETA = (3.0, 2.0, 1.0)
+N, STEPS = 100_000, 2000
+
+
+def test_adjoint_at_config_size(lmb):
+    W, capi = lmb.workloads, lmb.capi
+    f = W.grid2p1_fields()
+
+    def workload(th, prec):
+        a, b, s = th
+        return W.adjoint_grid(N=N, steps=STEPS, fields=f, a=a, b=b, scale=s, precision=prec)
+
+    base = capi.Engine(0)
+    wl = workload(THETA, "fp32")
+    assert abs(wl.params["dt"] * STEPS - 9.4) < 1e-9          # the grid's tau range exactly
+    W.configure(base, wl)
+    base.initial_lab_boost()
+    obs, G = base.adjoint(1, STEPS, checkpoint_every=64)
+
+    def run_at(th):
+        e = capi.Engine(0)
+        W.configure(e, workload(th, "fp64"))
+        e.initial_lab_boost()
+        e.copy_rta_decisions(base)
+        e.run(1, STEPS)
+        o = observables(e.download_state()[1])
+        e.close()
+        return o
+
+    FD, FD2 = central_differences(run_at)
+    base.close()
+    err_h, err, fd_err = compare("config size (201x201x100, 1e5 charm, 2000 steps)", G, FD, FD2, obs)
+    settled = fd_err < 1e-4
+    print(f"settled entries {int(settled.sum())}/9; max error vs FD(h) there "
+          f"{err_h[settled].max() if settled.any() else 0:.3g}")
+    assert np.all(err_h[settled] <= 1e-3)
+    assert np.all(err <= 1e-3 + 2 * fd_err)

@@ -6,9 +6,9 @@ Metric: per particle ||a - b|| / max(||b||, floor * s), s = 0.3 GeV for momenta 
   FP64 gate 1e-12 with floor 1e-2 (relative down to 3 MeV / 0.01 fm: a momentum that
   passes through zero, as the signed radial one does, keeps the ~1e-15 GeV absolute
   rounding it gathered at the GeV scale).
-  FP32 gate 1e-5 with floor 1: FP32 arithmetic errs by ~eps * E in absolute terms,
-  so it is gated at the natural momentum and length scales; the strict (floor
-  1e-3) figure is printed beside it.
+  FP32 gate 1e-5 with floor 1e-3 (0.3 MeV, 1 um), the two cases of FP32_FLOOR_CASE at a
+  larger floor for the reasons given there.  Freeze-out outputs: the one-step split of
+  check_latch_one_step.
 RTA accept/reject decisions must be identical: a flipped decision moves a momentum
 by O(1) and fails either gate."""
 import numpy as np
@@ -20,7 +20,15 @@ from parity_cases import CASES, build_case
 pytestmark = pytest.mark.gpu
 
 TOL = {"fp64": 1e-12, "fp32": 1e-5}
-FP32_FLOOR = 1.0
+FP32_FLOOR = 1e-3
+# Cases whose FP32 error relative to a 1e-3 floor (0.3 MeV, 1 um) exceeds 1e-5 for a
+# stated reason, gated at a larger floor (the 1e-3 figure is printed for them too):
+#   radial_diffusion_reflect: the 1-D signed radial momentum passes through zero, so a
+#     component of ~0.3 MeV carries the ~1e-9 GeV absolute error of the GeV scale;
+#   flow2d_v2: the flow speed is modulated by cos 2(phi - psi2) of the particle's FP32
+#     azimuth (atan2f, cosf), an FP32 error of the local frame that particles near p = 0
+#     show at the 1e-5 level against the strict floor.
+FP32_FLOOR_CASE = {"radial_diffusion_reflect": 1.0, "flow2d_v2": 1e-2}
 
 
 def engine_run(lmb, wl, *, record=False, save_every=0, nslots=0, split=None):
@@ -117,7 +125,7 @@ def check_fo_outputs(lmb, orc, wl, name, record):
     o = oracle_run(orc, wl, g["x0"], g["p0"], rec=g.get("rec"), precision=1)
     tag = f"{name} fp32/{'rec' if record else 'philox'}"
     if "fo" not in g:
-        assert_parity(tag, g, o, TOL["fp32"], floor=FP32_FLOOR)
+        assert_parity(tag, g, o, TOL["fp32"], floor=FP32_FLOOR_CASE.get(name, FP32_FLOOR))
         return
     gf, of = g["fo"]["flag"], o["fo_flag"]
     assert np.mean(gf == of) >= 0.999, np.mean(gf == of)
@@ -138,8 +146,9 @@ def check_latch_one_step(tag, wl, g, o, both):
         crossing) at the FP32 tolerance, and the engine's output equals the oracle's
         interpolation taken with the engine's frac (read off its latched tau) at the
         FP32 tolerance;
-      - the frac difference is that of a crossing-temperature difference below
-        2e-6 GeV (frac_e's implied T_b against the oracle's).
+      - the frac difference is that of temperature differences below 2e-6 GeV: with
+        frac = (T_a - Tfo)/(T_a - T_b), errors dT in T_a and T_b move frac by at most
+        dT / (T_a - T_b), so |frac_e - frac_o| (T_a - T_b) is gated.
     Runs without stop_after_freezeout keep moving after the latch (no crossing state
     to compare): their latch outputs are gated by the frac split alone."""
     if not np.any(both):
@@ -154,8 +163,7 @@ def check_latch_one_step(tag, wl, g, o, both):
     assert np.mean(same_step) >= 0.999, np.mean(same_step)
     k = same_step & has_last & (frac_o > 1e-6)
     Tb_o = lT[k] - (lT[k] - Tfo) / frac_o[k]
-    Tb_e = lT[k] - (lT[k] - Tfo) / np.clip(frac_e[k], 1e-12, None)
-    dT = np.abs(Tb_e - Tb_o)
+    dT = np.abs(frac_e[k] - frac_o[k]) * (lT[k] - Tb_o)
     a_x, a_p = o["fo_lpos"][:, both][:, k], o["fo_lmom"][:, both][:, k]
     if stop:
         b_x, b_p = o["x"][:, both][:, k], o["p"][:, both][:, k]
@@ -169,7 +177,7 @@ def check_latch_one_step(tag, wl, g, o, both):
         eb = er = 0.0
     ep = parity(g["fo"]["mom"][:, both], o["fo_mom"][:, both], 0.3, FP32_FLOOR)
     print(f"{tag} latched ({int(k.sum())}): crossing state {eb:.3g}, output at the engine's frac {er:.3g}, "
-          f"crossing temperature max {dT.max() if dT.size else 0:.3g} GeV; raw latched momentum max {ep[0]:.3g} "
+          f"temperature-equivalent frac difference max {dT.max() if dT.size else 0:.3g} GeV; raw latched momentum max {ep[0]:.3g} "
           f"p99 {ep[1]:.3g}")
     assert eb <= TOL["fp32"] and er <= TOL["fp32"], (tag, eb, er)
     assert dT.size == 0 or dT.max() <= 2e-6, (tag, dT.max())
