@@ -36,11 +36,12 @@ k_cart(const KParams<R> kp, int64_t s0, int64_t s1)
     cart_particle<REC, FO, R, MED, DIMS, PDIM>(kp, kp.rk, i, s0, s1);
 }
 
-// The FP32 grid kernel with the freeze-out latch, held to 85 registers so that three
-// 256-thread blocks stay resident per SM (7 % faster than its natural 92 registers on
-// the 2+1D workload; the other instantiations lose by such a cap).
+// The FP32 grid kernel with the freeze-out latch, in blocks of 128 held to 72 registers
+// so that seven blocks stay resident per SM (1.3 % faster on the 2+1D workloads than
+// three blocks of 256 at 80 registers, 13 % faster than two at 128; the other
+// instantiations lose by such a cap).
 template <bool REC, int DIMS, int PDIM>
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(128, 7)
 k_cart_grid_fo32(const KParams<float> kp, int64_t s0, int64_t s1)
 {
     if (kp.live) {
@@ -142,7 +143,7 @@ static cudaError_t launch_cart_fo(const KParams<R>& kp, int64_t s0, int64_t s1, 
     const int dp = kp.dims * 10 + kp.pdim;
     if (MED == MED_GRID) {
         if constexpr (FO && sizeof(R) == 4) {
-            if (block <= 256) {
+            if (block <= 128) {
                 const KParams<float>& kf = reinterpret_cast<const KParams<float>&>(kp);
                 if (dp == 22) k_cart_grid_fo32<REC, 2, 2><<<g, block, 0, st>>>(kf, s0, s1);
                 else if (dp == 23) k_cart_grid_fo32<REC, 2, 3><<<g, block, 0, st>>>(kf, s0, s1);

@@ -26,9 +26,9 @@ FP32_FLOOR = 1e-3
 #   radial_diffusion_reflect: the 1-D signed radial momentum passes through zero, so a
 #     component of ~0.3 MeV carries the ~1e-9 GeV absolute error of the GeV scale;
 #   flow2d_v2: the flow speed is modulated by cos 2(phi - psi2) of the particle's FP32
-#     azimuth (atan2f, cosf), an FP32 error of the local frame that particles near p = 0
-#     show at the 1e-5 level against the strict floor.
-FP32_FLOOR_CASE = {"radial_diffusion_reflect": 1.0, "flow2d_v2": 1e-2}
+#     azimuth (atan2f, cosf); the frame change then carries an absolute error of order
+#     eps_32 E ~ 1e-7 GeV, which particles slower than ~30 MeV show above 1e-5 relative.
+FP32_FLOOR_CASE = {"radial_diffusion_reflect": 1.0, "flow2d_v2": 0.1}
 
 
 def engine_run(lmb, wl, *, record=False, save_every=0, nslots=0, split=None):
