@@ -52,6 +52,7 @@ METRIC = "particle-steps/s on 1 B200 (plain vs batched; fwd+adjoint cost) at ≤
 WORKLOAD = "grid2p1_langevin_rta_fo_5e6c_5e6b_fp32"
 SPECIES = ((1.5, "charm"), (4.75, "bottom"))
 HBM_FALLBACK_GBS = 6650.0
+LIVE_SUBCHUNK_STEPS = 32          # steps per launch of a stop-at-freeze-out run (the live list's sub-chunk)
 
 
 def load_package():
@@ -426,11 +427,19 @@ def per_pipe_roofline(counts, fma_rate, mufu_rate, particle_steps, kernel_s):
             "note": "XU count includes the conversions; ALU/FP64/LSU rates nominal ratios of the measured FMA rate"}
 
 
-def issue_roofline(pkg, key, fma_rate, mufu_rate, particle_steps, seconds, n_particles, launches):
+def issue_roofline(pkg, key, fma_rate, mufu_rate, particle_steps, seconds, n_particles, launches,
+                   live_steps=None):
+    """launches: step-kernel launches per particle over the pass; live_steps: for runs on
+    a compacted live list, the steps of one sub-chunk launch (each launch reads and
+    writes the state of the particles live in it once, so the algorithmic bytes are the
+    per-launch figure per live particle times executed particle-steps / live_steps)."""
     counts, i_alg, hbm_pp = work_counts(pkg, key)
     achieved = i_alg * particle_steps / seconds
     peaks, src = measured_peaks()
-    bytes_total = hbm_pp * n_particles * max(1, launches)
+    if live_steps:
+        bytes_total = hbm_pp * particle_steps / live_steps
+    else:
+        bytes_total = hbm_pp * n_particles * max(1, launches)
     return {
         "bound": "issue", "unit": "Ginst/s", "achieved": achieved / 1e9, "peak": fma_rate / 1e9,
         "frac": achieved / fma_rate, "traffic": None,
@@ -729,7 +738,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     eng0.close()
     pass_s = (total_ms / args.steps) * 1e-3
     roofline = issue_roofline(pkg, "grid2p1_langevin_rta_fo_fp32", fma_rate, mufu_rate, executed / world, pass_s,
-                              h["n"], max(1, h["launches"] // max(1, args.steps) // 2))
+                              h["n"], 0, live_steps=LIVE_SUBCHUNK_STEPS)
     roofline["kernel"] = ("k_cart_grid_fo32 (fused Langevin+RTA step with the freeze-out latch, sub-chunks of 32 "
                           "steps over a compacted live list; two species on two streams)")
     roofline["timing"] = ("achieved: algorithmic instructions of the executed particle-steps / the device span of a "
