@@ -289,7 +289,12 @@ def accuracy_against_cpu(pkg, samples, cpu_outs) -> dict:
     against the restatement's FP64 result.  Per particle ||a - b|| / max(||b||, f s),
     s = 0.3 GeV for momenta and 1 fm for positions and times, f = 1e-3 (the strict
     floor) and 1: the final state of particles live in both runs, the freeze-out
-    outputs (position, momentum, tau) of particles latched in both."""
+    outputs (position, momentum, tau) of particles latched in both; a particle's error
+    is the largest of its quantities'.  A particle off by more than 1e-2 (floor 1) has
+    diverged: a decision (an RTA collision, a freeze-out crossing) fell within the two
+    trajectories' difference of its threshold and went the other way, after which the
+    trajectories are different draws.  Those are counted, and the maxima are also
+    given over the particles that did not diverge."""
     W, capi = pkg.workloads, pkg.capi
     res = {"sample": f"{samples[0].n} charm + {samples[1].n} bottom quarks of the headline workload, 940 steps",
            "metric": "per-particle relative error, max / 99.99th / 99th percentile"}
@@ -310,16 +315,28 @@ def accuracy_against_cpu(pkg, samples, cpu_outs) -> dict:
             flips += int(np.sum(gf != of))
             live, both = (gf == 0) & (of == 0), (gf == 1) & (of == 1)
             for fl in errs:
-                errs[fl]["live"] += [per_particle_err(p[:, live], o["p"][:, live], 0.3, fl),
-                                     per_particle_err(x[:, live], o["x"][:, live], 1.0, fl)]
-                errs[fl]["latch"] += [per_particle_err(f["mom"][:, both], o["fo_mom"][:, both], 0.3, fl),
-                                      per_particle_err(f["pos"][:, both], o["fo_pos"][:, both], 1.0, fl),
-                                      per_particle_err(f["tau"][both], o["fo_tau"][both], 1.0, fl)]
+                errs[fl]["live"].append(np.maximum(per_particle_err(p[:, live], o["p"][:, live], 0.3, fl),
+                                                   per_particle_err(x[:, live], o["x"][:, live], 1.0, fl)))
+                errs[fl]["latch"].append(np.maximum.reduce([
+                    per_particle_err(f["mom"][:, both], o["fo_mom"][:, both], 0.3, fl),
+                    per_particle_err(f["pos"][:, both], o["fo_pos"][:, both], 1.0, fl),
+                    per_particle_err(f["tau"][both], o["fo_tau"][both], 1.0, fl)]))
         out = {"freezeout_flag_mismatches": flips}
+        kept = {}
+        for k in ("live", "latch"):
+            e1 = np.concatenate(errs[1.0][k]) if errs[1.0][k] else np.zeros(0)
+            kept[k] = e1 <= 1e-2
+            out[f"diverged_{k}"] = int((~kept[k]).sum())
         for fl, d in errs.items():
             for k, parts in d.items():
-                e = np.concatenate([q for q in parts if q.size]) if any(q.size for q in parts) else np.zeros(1)
+                e = np.concatenate(parts) if parts else np.zeros(0)
+                if e.size == 0:
+                    e = np.zeros(1)
+                    ok = np.ones(1, bool)
+                else:
+                    ok = kept[k]
                 out[f"{k}_floor{fl:g}"] = [float(e.max()), float(np.percentile(e, 99.99)), float(np.percentile(e, 99))]
+                out[f"{k}_floor{fl:g}_max_not_diverged"] = float(e[ok].max()) if ok.any() else 0.0
         res[f"{prec}_vs_fp64_cpu"] = out
     return res
 
