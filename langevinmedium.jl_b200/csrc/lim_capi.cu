@@ -246,6 +246,12 @@ int build_kparams(lim_ctx* c, KParams<R>& kp)
         md.gx0_d = c->gx0; md.gdx_d = c->gdx; md.gxl_d = c->gx0 + (double)(c->gnx - 1) * c->gdx;
         md.gy0_d = c->gy0; md.gdy_d = c->gdy; md.gyl_d = c->gy0 + (double)(c->gny - 1) * c->gdy;
         md.ginvdx = (float)(1.0 / c->gdx); md.ginvdy = (float)(1.0 / c->gdy);
+        md.ginvdx_lo = (float)(1.0 / c->gdx - (double)md.ginvdx);
+        md.ginvdy_lo = (float)(1.0 / c->gdy - (double)md.ginvdy);
+        md.gicx = (int)((c->gnx - 1) / 2); md.gicy = (int)((c->gny - 1) / 2);
+        const double xcd = c->gx0 + (double)md.gicx * c->gdx, ycd = c->gy0 + (double)md.gicy * c->gdy;
+        md.gxc = (float)xcd; md.gxcl = (float)(xcd - (double)md.gxc);
+        md.gyc = (float)ycd; md.gycl = (float)(ycd - (double)md.gyc);
         md.gt0 = c->gt0; md.gdt_d = c->gdt; md.gtl = c->gt0 + (double)(c->gnt - 1) * c->gdt;
         double r = std::fabs(md.gx0_d);
         r = std::min(r, std::fabs(md.gxl_d)); r = std::min(r, std::fabs(md.gy0_d)); r = std::min(r, std::fabs(md.gyl_d));

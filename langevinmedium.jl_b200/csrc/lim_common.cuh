@@ -55,6 +55,10 @@ struct MediumDev {
     const float4* G; int gnx, gny, gnt;
     double gx0_d, gdx_d, gxl_d, gy0_d, gdy_d, gyl_d;   // node geometry (FP64)
     float ginvdx, ginvdy;                              // FP32 fast path
+    // FP32 cell location: the node nearest the grid's centre (index, coordinate as a
+    // float pair) and the low words of 1/dx, 1/dy
+    int gicx, gicy;
+    float gxc, gxcl, gyc, gycl, ginvdx_lo, ginvdy_lo;
     double gt0, gdt_d, gtl;
     // geometry of the reflecting boundary (kernels_cpu.jl:528-534)
     R r_max, r_axis_eps;

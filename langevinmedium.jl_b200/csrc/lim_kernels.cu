@@ -118,7 +118,7 @@ k_lab_boost(const KParams<R> kp)
     float xl[3];
     load_state<R, DIMS, PDIM>(kp, i, x, xl, p);
     const StepRec<R> sr = make_step_rec<R, MED>(kp, 0);
-    const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x);
+    const Local<R> L = local_medium<R, MED, DIMS>(kp, sr, x, nullptr, nullptr, xl);
     if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) kp.p[d][i] = p[d];

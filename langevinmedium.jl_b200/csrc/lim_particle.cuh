@@ -104,7 +104,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     GridRows<R> rows;
     rows.kt = -1;
     GridRows<R>* carry = kCarry ? &rows : nullptr;
-    if (kCarry && s0 < s1) grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows);
+    if (kCarry && s0 < s1) grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows, xl[0], xl[1]);
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && frozen) break;
         const StepRec<R> sr = tab[s];
@@ -119,7 +119,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             // the next step's time row: from the table inside the launch, computed past it
             double w;
             const int kn = s + 1 < s1 ? tab[s + 1].kt : grid_time_cell(kp.med, step_time(kp, s + 1), w);
-            grid_rows(kp.med, kn, x[0], x[1], rows);
+            grid_rows(kp.med, kn, x[0], x[1], rows, xl[0], xl[1]);
         }
         if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last,
                                                     carry);

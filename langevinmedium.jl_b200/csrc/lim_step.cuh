@@ -156,29 +156,66 @@ __device__ __forceinline__ R rt_lookup_scalar(const MediumDev<R>& md, const Step
     return c0 * (R(1) - yd) + c1 * yd;
 }
 
-// 2+1D grid: trilinear of (T, ux, uy) at (x, y) clamped to the grid.  The
-// FP32 path finds the cell in FP32; the FP64 path in FP64 from the same nodes.
+// FP32 cell index i and weight w of the clamped coordinate q (low word ql) on a uniform
+// axis of n nodes: the coordinate is taken relative to the node ic nearest the axis's
+// centre (xc + xcl as a float pair) and scaled by 1/dx (inv + ilo), keeping the
+// rounding of both steps (TwoSum of q - xc, the exact FMA remainder of the product), so
+// the weight is the cell fraction rounded once.  Measured from the far origin instead,
+// (q - x0) / dx rounds at the ulp of ~100 cells: a weight error of up to 1e-5, which the
+// momentum of a slow heavy quark in a flowing cell follows (FP32 against FP64 per
+// particle 1.1e-5 before, 3.6e-6 after, on the 201 x 201 grid of 0.1 fm).
+__device__ __forceinline__ void cell_fp32(float q, float ql, int ic, float xc, float xcl, float inv, float ilo,
+                                          int n, int& i, float& w)
+{
+    const float s = __fsub_rn(q, xc);
+    const float bp = __fsub_rn(s, q);
+    const float err = __fadd_rn(__fsub_rn(q, __fsub_rn(s, bp)), __fsub_rn(-xc, bp));
+    const float dlo = __fadd_rn(__fsub_rn(err, xcl), ql);
+    const float pr = __fmul_rn(s, inv);
+    const float e = __fmaf_rn(s, inv, -pr);
+    const float lo = __fadd_rn(e, __fmaf_rn(s, ilo, __fmul_rn(dlo, inv)));
+    const float fl = floorf(pr);
+    int k = ic + (int)fl;                // (int) of NaN is 0: the index stays on the grid
+    float base = fl;
+    if (k < 0) { k = 0; base = (float)(-ic); }
+    if (k > n - 2) { k = n - 2; base = (float)(n - 2 - ic); }
+    i = k;
+    w = __fadd_rn(__fsub_rn(pr, base), lo);
+}
+
+// 2+1D grid: trilinear of (T, ux, uy) at (x, y) clamped to the grid.  The FP32 path
+// finds the cell with cell_fp32 (xlo, ylo: the position's low words, dropped where the
+// query is clamped); the FP64 path in FP64 from the same nodes.
 template <typename R>
-__device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, int& ix, int& iy, R& wx, R& wy)
+__device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, int& ix, int& iy, R& wx, R& wy,
+                                          float xlo = 0.0f, float ylo = 0.0f)
 {
     R x = xq > (R)md.gxl_d ? (R)md.gxl_d : (xq < (R)md.gx0_d ? (R)md.gx0_d : xq);
     R y = yq > (R)md.gyl_d ? (R)md.gyl_d : (yq < (R)md.gy0_d ? (R)md.gy0_d : yq);
-    R fx, fy;
-    if (sizeof(R) == 8) { fx = (x - (R)md.gx0_d) / (R)md.gdx_d; fy = (y - (R)md.gy0_d) / (R)md.gdy_d; }
-    else { fx = __fmul_rn(x - (R)md.gx0_d, (R)md.ginvdx); fy = __fmul_rn(y - (R)md.gy0_d, (R)md.ginvdy); }
-    R flx = floor(fx), fly = floor(fy);
-    ix = flx < R(0) ? 0 : (flx > R(md.gnx - 2) ? md.gnx - 2 : (int)flx);
-    iy = fly < R(0) ? 0 : (fly > R(md.gny - 2) ? md.gny - 2 : (int)fly);
-    wx = fx - R(ix);
-    wy = fy - R(iy);
+    if constexpr (sizeof(R) == 4) {
+        float fwx, fwy;
+        cell_fp32(x, x == xq ? xlo : 0.0f, md.gicx, md.gxc, md.gxcl, md.ginvdx, md.ginvdx_lo, md.gnx, ix, fwx);
+        cell_fp32(y, y == yq ? ylo : 0.0f, md.gicy, md.gyc, md.gycl, md.ginvdy, md.ginvdy_lo, md.gny, iy, fwy);
+        wx = fwx;
+        wy = fwy;
+    } else {
+        R fx = (x - (R)md.gx0_d) / (R)md.gdx_d, fy = (y - (R)md.gy0_d) / (R)md.gdy_d;
+        R flx = floor(fx), fly = floor(fy);
+        ix = flx < R(0) ? 0 : (flx > R(md.gnx - 2) ? md.gnx - 2 : (int)flx);
+        iy = fly < R(0) ? 0 : (fly > R(md.gny - 2) ? md.gny - 2 : (int)fly);
+        wx = fx - R(ix);
+        wy = fy - R(iy);
+    }
 }
 
-// a (1 - w) + b w as one product and one fused multiply-add, the rounding spelled out:
-// the compiler may not contract it differently where it is inlined, so the grid's
-// interpolation gives the same bits in every kernel and at every call site.
+// Linear interpolation with the rounding spelled out, so the compiler may not contract
+// it differently where it is inlined and the grid's interpolation gives the same bits in
+// every kernel and at every call site.  FP32: a + w (b - a) as one subtraction and one
+// fused multiply-add (b - a is exact for neighbouring nodes within a factor 2 of each
+// other, so the result is rounded once); FP64: the reference's a (1 - w) + b w.
 __device__ __forceinline__ float lerp_rn(float a, float b, float w)
 {
-    return __fmaf_rn(b, w, __fmul_rn(a, __fsub_rn(1.0f, w)));
+    return __fmaf_rn(w, __fsub_rn(b, a), a);
 }
 __device__ __forceinline__ double lerp_rn(double a, double b, double w)
 {
@@ -205,10 +242,10 @@ struct GridRows {
 // order 00, 10, 01, 11 (x fastest), and the cell weights.
 template <typename R>
 __device__ __forceinline__ void grid_corners(const MediumDev<R>& md, int kt, R xq, R yq, float4 (&a)[4],
-                                             float4 (&b)[4], R& Wx, R& Wy)
+                                             float4 (&b)[4], R& Wx, R& Wy, float xlo = 0.0f, float ylo = 0.0f)
 {
     int ix, iy;
-    grid_cell(md, xq, yq, ix, iy, Wx, Wy);
+    grid_cell(md, xq, yq, ix, iy, Wx, Wy, xlo, ylo);
     const float4* s0 = md.G + ((size_t)kt * md.gny + iy) * md.gnx + ix;
     const float4* s1 = s0 + (size_t)md.gny * md.gnx;
     a[0] = __ldg(s0); a[1] = __ldg(s0 + 1); a[2] = __ldg(s0 + md.gnx); a[3] = __ldg(s0 + md.gnx + 1);
@@ -224,11 +261,12 @@ __device__ __forceinline__ void rows_of(const float4 (&a)[4], const float4 (&b)[
 }
 
 template <typename R>
-__device__ __forceinline__ void grid_rows(const MediumDev<R>& md, int kt, R xq, R yq, GridRows<R>& g)
+__device__ __forceinline__ void grid_rows(const MediumDev<R>& md, int kt, R xq, R yq, GridRows<R>& g,
+                                          float xlo = 0.0f, float ylo = 0.0f)
 {
     float4 a[4], b[4];
     R Wx, Wy;
-    grid_corners(md, kt, xq, yq, a, b, Wx, Wy);
+    grid_corners(md, kt, xq, yq, a, b, Wx, Wy, xlo, ylo);
     rows_of(a, b, Wx, Wy, g);
     g.kt = kt;
 }
@@ -250,11 +288,11 @@ struct MedGrad {
 
 template <typename R, bool GRAD = false>
 __device__ __forceinline__ void grid_lookup(const MediumDev<R>& md, const StepRec<R>& sr, R xq, R yq, R& T, R& ux, R& uy,
-                                            MedGrad* mg = nullptr)
+                                            MedGrad* mg = nullptr, float xlo = 0.0f, float ylo = 0.0f)
 {
     float4 a[4], b[4];
     R Wx, Wy;
-    grid_corners(md, sr.kt, xq, yq, a, b, Wx, Wy);
+    grid_corners(md, sr.kt, xq, yq, a, b, Wx, Wy, xlo, ylo);
     const R Wt = sr.wt;
     GridRows<R> g;
     rows_of(a, b, Wx, Wy, g);
@@ -294,7 +332,8 @@ struct Local {
 
 template <typename R, int MED, int DIMS, bool GRAD = false>
 __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const StepRec<R>& sr, const R (&x)[3],
-                                                 MedGrad* mg = nullptr, GridRows<R>* carry = nullptr)
+                                                 MedGrad* mg = nullptr, GridRows<R>* carry = nullptr,
+                                                 const float* xl = nullptr)
 {
     constexpr bool fp32 = sizeof(R) == 4;
     Local<R> L;
@@ -305,7 +344,7 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
         if (!GRAD && carry) {                 // the rows of this step's time row at x
             grid_combine(*carry, sr.wt, L.T, ux, uy);
         } else {
-            grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg);
+            grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg, xl ? xl[0] : 0.0f, xl ? xl[1] : 0.0f);
         }
         R u = sqrt(ux * ux + uy * uy);
         L.boost = !(u < R(kEps));
@@ -767,7 +806,7 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
     MedGrad mg;
     float4* trow = nullptr;
     if constexpr (kTapeGrid) trow = reinterpret_cast<float4*>(kp.tape) + (s - kp.tape_first) * 4 * kp.n + i;
-    const Local<R> L = local_medium<R, MED, DIMS, kTapeGrid>(kp, sr, x, &mg, carry);
+    const Local<R> L = local_medium<R, MED, DIMS, kTapeGrid>(kp, sr, x, &mg, carry, xl);
     if constexpr (kTapeGrid) {
         trow[0] = make_float4((float)p[0], (float)p[1], (float)p[2], mg.T);
         trow[2 * kp.n] = make_float4(mg.vy, mg.dT[0], mg.dT[1], mg.dvx[0]);
