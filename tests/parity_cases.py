@@ -49,7 +49,8 @@ def initial(rng, N, dims, pdim, spread=4.0, pmax=4.0):
 
 CASES = ["static3d", "flow2d", "flow2d_nonrel", "flow2d_v2", "flow2d_midpoint", "flow2d_nonuniform",
          "flow3d", "rta2d", "lrta_bjorken_table", "fluid_redshift", "radial_diffusion_reflect",
-         "cart_diffusion_reflect", "freezeout", "milne", "bjorken_analytic", "grid_lrta_fo", "grid_fine_tau_fo"]
+         "cart_diffusion_reflect", "freezeout", "milne", "bjorken_analytic", "grid_lrta_fo", "grid_fine_tau_fo",
+         "grid_offset_fo"]
 
 
 def build_case(name: str, precision: str = "fp64", N: int = 2048, steps: int | None = None, seed: int = 7):
@@ -121,5 +122,14 @@ def build_case(name: str, precision: str = "fp64", N: int = 2048, steps: int | N
         # time row, so the FP32 kernel's latch screen never reuses the step's lookup
         f = W.grid2p1_fields(nx=41, ny=41, nt=160, dx=0.5, tau0=0.6, tauf=3.0, sx=3.0, sy=2.4)
         wl = W.grid2p1(N=N, precision=precision, fields=f, steps=steps or 110, seed=seed, dt=0.02)
+        return wl
+    if name == "grid_offset_fo":
+        # an even node count, a spacing whose reciprocal FP32 does not hold exactly and a
+        # grid shifted off the particles' centre: the FP32 cell location's centre node
+        # (index 31 of 64) is not at 0, so its TwoSum and low-word terms are all non-zero
+        f = W.grid2p1_fields(nx=64, ny=57, nt=24, dx=0.3, sx=3.0, sy=2.4)
+        f["x0"] += 1.37
+        f["y0"] -= 0.61
+        wl = W.grid2p1(N=N, precision=precision, fields=f, steps=steps or 300, seed=seed, dt=0.02)
         return wl
     raise KeyError(name)

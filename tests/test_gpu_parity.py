@@ -109,7 +109,8 @@ def test_fp32_parity_recorded_noise(lmb, orc, name):
     check_fo_outputs(lmb, orc, wl, name, record=True)
 
 
-@pytest.mark.parametrize("name", ["static3d", "lrta_bjorken_table", "grid_lrta_fo", "grid_fine_tau_fo", "milne"])
+@pytest.mark.parametrize("name", ["static3d", "lrta_bjorken_table", "grid_lrta_fo", "grid_fine_tau_fo", "grid_offset_fo",
+                                  "milne"])
 def test_fp32_parity_philox(lmb, orc, name):
     """FP32 engine vs FP64 restatement regenerating the FP32 uniforms from Philox
     (the whole FP32 error: arithmetic plus the FP32 noise transform)."""
