@@ -87,9 +87,10 @@ class _PinnedBlock:
             raise LimError(rc, lib.lim_last_error(None).decode())
 
     def __del__(self):
-        if self.ptr and self.ptr.value:
-            self.lib.lim_host_free(self.ptr)
-            self.ptr = C.c_void_p()
+        # at interpreter exit module globals (ctypes included) may already be gone
+        ptr, self.ptr = getattr(self, "ptr", None), None
+        if ptr is not None and ptr.value:
+            self.lib.lim_host_free(ptr)
 
 
 def pinned_empty(n: int, dtype=np.float64, lib: C.CDLL | None = None) -> np.ndarray:
