@@ -46,6 +46,46 @@ def test_fp32_vs_fp64_bjorken_full_size(lmb):
         assert math.isclose(o32[k], o64[k], rel_tol=1e-5)
 
 
+@pytest.mark.parametrize("m", [1.5, 4.75])
+def test_fp32_vs_fp64_grid_freezeout(lmb, m):
+    """The headline workload's configuration (201 x 201 x 100 grid, Langevin + RTA,
+    freeze-out latch, particles stop; 940 steps) on 2e5 charm or bottom quarks, FP32
+    against FP64 on the same noise: live particles' final state and the latched
+    particles' freeze-out outputs.  A particle whose error is O(1e-2) or more has
+    diverged (a decision fell within the two trajectories' rounding difference of its
+    threshold; about one per 1e6 particles per run): at most one.  The others: live
+    state <= 1e-5 per particle (floor 1: 0.3 GeV, 1 fm); latched outputs, ill-conditioned
+    where a trajectory grazes the isotherm, p99.99 <= 2e-4; no freeze-out flag may
+    differ."""
+    W = lmb.workloads
+    f = W.grid2p1_fields()
+    out = {}
+    for prec in ("fp32", "fp64"):
+        wl = W.grid2p1(N=200_000, m=m, fields=f, precision=prec, rng_seed=21)
+        eng = lmb.capi.Engine(0)
+        W.configure(eng, wl)
+        eng.initial_lab_boost()
+        eng.run(wl.first_step, wl.steps)
+        x, p = eng.download_state()
+        out[prec] = (x, p, eng.download_freezeout())
+        eng.close()
+    (x32, p32, f32), (x64, p64, f64) = out["fp32"], out["fp64"]
+    assert np.array_equal(f32["flag"], f64["flag"])
+    live, lat = f64["flag"] == 0, f64["flag"] == 1
+    rel = lambda a, b, s: np.linalg.norm(a - b, axis=0) / np.maximum(np.linalg.norm(b, axis=0), s)
+    el = np.maximum(rel(p32[:, live], p64[:, live], 0.3), rel(x32[:, live], x64[:, live], 1.0))
+    ef = np.maximum.reduce([rel(f32["mom"][:, lat], f64["mom"][:, lat], 0.3),
+                            rel(f32["pos"][:, lat], f64["pos"][:, lat], 1.0),
+                            np.abs(f32["tau"][lat] - f64["tau"][lat]) / np.maximum(f64["tau"][lat], 1.0)])
+    diverged = int(np.count_nonzero(el > 1e-2) + np.count_nonzero(ef > 1e-2))
+    el, ef = el[el <= 1e-2], ef[ef <= 1e-2]
+    print(f"m={m}: live {el.size} max {el.max():.3g} p99.99 {np.percentile(el, 99.99):.3g}; latched {ef.size} "
+          f"max {ef.max():.3g} p99.99 {np.percentile(ef, 99.99):.3g}; diverged {diverged}")
+    assert diverged <= 1
+    assert el.max() <= 1e-5
+    assert np.percentile(ef, 99.99) <= 2e-4
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 def test_bjorken_telescoping_full_size(lmb, prec):
     """kernels_cpu.jl:427-435 with momentum_langevin=false: <p_z^2>(tau) = <p_z^2>(tau0)(tau0/tau)^2."""
