@@ -168,9 +168,18 @@ __device__ __forceinline__ SplIdx<R> spline_index(R T, R Tmin, R invdT, int n)
     if (!isfinite(T)) { s.mode = 2; return s; }
     s.mode = 0;
     R u = (T - Tmin) * invdT;
-    R fl = floor(u);
-    s.i = fl < R(0) ? 0 : (fl > R(n - 2) ? n - 2 : (int)fl);
-    s.t = u - R(s.i);
+    if constexpr (sizeof(R) == 4) {
+        // floor(u) from one round-down add of 1.5 2^23 (exact for |u| < 2^22; beyond the
+        // clamp the index is clamped to the table either way): no FP32 -> int conversion
+        const float tf = __fadd_rd(jclamp(u, -4.0e6f, 4.0e6f), 12582912.0f);
+        const int k = __float_as_int(tf) - 0x4B400000;
+        s.i = k < 0 ? 0 : (k > n - 2 ? n - 2 : k);
+        s.t = __fmaf_rn(T - Tmin, invdT, -(float)s.i);   // fused: one rounding in every instantiation
+    } else {
+        R fl = floor(u);
+        s.i = fl < R(0) ? 0 : (fl > R(n - 2) ? n - 2 : (int)fl);
+        s.t = u - R(s.i);
+    }
     return s;
 }
 

@@ -96,15 +96,21 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
     // FP32 grid runs with the freeze-out latch: one spatial lookup per step, at the end
-    // of the step for the next step's time row, serves both the next step and the
-    // latch's screen.  The first step's rows are looked up here; every step then takes
-    // its medium from the same code whether or not a launch boundary falls before it,
-    // so a run split into more launches gives the same bits.
+    // of the step at the new position on the next step's time row, serves both the next
+    // step (its medium, blended in time at once into rows.T0, U0, V0) and the latch's
+    // screen (rows.T1).  The first step's medium is looked up here, and the last step of
+    // a launch looks up its own time row for the screen only; every step takes its
+    // medium from the same code whether or not a launch boundary falls before it, so a
+    // run split into more launches gives the same bits.
     constexpr bool kCarry = FO && MED == MED_GRID && sizeof(R) == 4;
     GridRows<R> rows;
     rows.kt = -1;
     GridRows<R>* carry = kCarry ? &rows : nullptr;
-    if (kCarry && s0 < s1) grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows, xl[0], xl[1]);
+    if (kCarry && s0 < s1) {
+        grid_rows(kp.med, tab[s0].kt, x[0], x[1], rows, xl[0], xl[1]);
+        const R w0 = tab[s0].wt;
+        grid_combine(rows, w0, rows.T0, rows.U0, rows.V0);
+    }
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && frozen) break;
         const StepRec<R> sr = tab[s];
@@ -116,10 +122,14 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
         float pf[3];
         cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
         if constexpr (kCarry) {
-            // the next step's time row: from the table inside the launch, computed past it
-            double w;
-            const int kn = s + 1 < s1 ? tab[s + 1].kt : grid_time_cell(kp.med, step_time(kp, s + 1), w);
+            const bool more = s + 1 < s1;
+            int kn = sr.kt;
+            R wn = R(0);
+            if (more) { kn = tab[s + 1].kt; wn = tab[s + 1].wt; }
             grid_rows(kp.med, kn, x[0], x[1], rows, xl[0], xl[1]);
+            const float scr = kn == sr.kt ? (float)lerp_rn(rows.T0, rows.T1, sr.wt) * (float)kp.med.T_scale : -1.0f;
+            if (more) grid_combine(rows, wn, rows.T0, rows.U0, rows.V0);
+            rows.T1 = scr;
         }
         if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last,
                                                     carry);

@@ -174,8 +174,11 @@ __device__ __forceinline__ void cell_fp32(float q, float ql, int ic, float xc, f
     const float pr = __fmul_rn(s, inv);
     const float e = __fmaf_rn(s, inv, -pr);
     const float lo = __fadd_rn(e, __fmaf_rn(s, ilo, __fmul_rn(dlo, inv)));
-    const float fl = floorf(pr);
-    int k = ic + (int)fl;                // (int) of NaN is 0: the index stays on the grid
+    // floor(pr) from one round-down add: for |pr| < 2^22 the low mantissa bits of
+    // pr + 1.5 2^23 rounded down hold floor(pr) (NaN gives a large index, clamped below)
+    const float tf = __fadd_rd(pr, 12582912.0f);
+    const float fl = __fsub_rn(tf, 12582912.0f);
+    int k = ic + (__float_as_int(tf) - 0x4B400000);
     float base = fl;
     if (k < 0) { k = 0; base = (float)(-ic); }
     if (k > n - 2) { k = n - 2; base = (float)(n - 2 - ic); }
@@ -208,6 +211,14 @@ __device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, in
     }
 }
 
+// Products and fused multiply-adds with their rounding spelled out, for expressions
+// with two products (a b + c d), where the compiler's contraction may otherwise pick a
+// different product to fuse in different instantiations of the same step.
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // Linear interpolation with the rounding spelled out, so the compiler may not contract
 // it differently where it is inlined and the grid's interpolation gives the same bits in
 // every kernel and at every call site.  FP32: a + w (b - a) as one subtraction and one
@@ -229,9 +240,11 @@ __device__ __forceinline__ R bilerp_rn(float a00, float a10, float a01, float a1
 
 // The grid at a position, interpolated in space only: (T, v^x, v^y) on time rows kt
 // (T0, U0, V0) and kt + 1 (T1, U1, V1), the two values grid_lookup blends in time.  The
-// freeze-out kernel looks them up once per step, at the end of step s for the time row
-// of step s + 1 at the new position: step s + 1 takes its medium from them, and the
-// latch of step s its temperature screen when the two steps share the time row.
+// FP32 freeze-out kernel looks them up once per step, at the end of step s at the new
+// position on the time row of step s + 1, and carries the result into step s + 1
+// (cart_particle): blended in time at once, T0, U0, V0 then hold the medium of step
+// s + 1 and T1 the latch's temperature screen of step s (-1 where the two steps do not
+// share the time row: the FP64 test decides), so four values stay live across the step.
 template <typename R>
 struct GridRows {
     R T0, T1, U0, U1, V0, V1;
@@ -341,12 +354,12 @@ __device__ __forceinline__ Local<R> local_medium(const KParams<R>& kp, const Ste
     if (MED == MED_GRID) {
         // the grid holds the flow velocity (v^x, v^y), as the reference's (r, t) tables do
         R ux, uy;
-        if (!GRAD && carry) {                 // the rows of this step's time row at x
-            grid_combine(*carry, sr.wt, L.T, ux, uy);
+        if (!GRAD && carry) {                 // looked up and blended at the end of the previous step
+            L.T = carry->T0; ux = carry->U0; uy = carry->V0;
         } else {
             grid_lookup<R, GRAD>(kp.med, sr, x[0], x[1], L.T, ux, uy, mg, xl ? xl[0] : 0.0f, xl ? xl[1] : 0.0f);
         }
-        R u = sqrt(ux * ux + uy * uy);
+        R u = sqrt(fma_rn(ux, ux, mul_rn(uy, uy)));
         L.boost = !(u < R(kEps));
         L.v = u;
         if (L.boost) { L.nx = ux / u; L.ny = uy / u; }
@@ -437,6 +450,23 @@ __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, d
     v = jclamp(v, -vmax, vmax);
     double gam = gamp;
     if (!(gam > 0.0)) gam = sizeof(R) == 4 ? rsqrt_f32_newton(1.0 - v * v + 1e-10) : 1.0 / sqrt(1.0 - v * v + 1e-10);
+    if constexpr (sizeof(R) == 4) {
+        if (DIMS >= 2) {
+            // p' = p + d n with d = p'_par - p_par = (gamma - 1) p_par +- gamma v E: the same
+            // frame change as the reference's split into parallel and perpendicular parts,
+            // in fewer FP64 operations (FP32 path only; the FP64 path keeps the reference's form)
+            double q = m * m;
+#pragma unroll
+            for (int d = PDIM - 1; d >= 0; --d) q = fma(p[d], p[d], q);
+            const double E = sqrt_f32_newton(q);
+            const double ppar = fma(p[0], nx, p[1] * ny);
+            const double gvE = (gam * v) * E;
+            const double dd = fma(gam - 1.0, ppar, to_lab ? gvE : -gvE);
+            p[0] = fma(dd, nx, p[0]);
+            p[1] = fma(dd, ny, p[1]);
+            return;
+        }
+    }
     double p2 = 0.0;
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) p2 += p[d] * p[d];
@@ -444,7 +474,7 @@ __device__ __forceinline__ void boost(const KParams<R>& kp, const Local<R>& L, d
     double vE = to_lab ? v * E : -(v * E);
     if (DIMS == 1) { p[0] = gam * (p[0] + vE); return; }
     double px = p[0], py = p[1];
-    double ppar = px * nx + py * ny;
+    double ppar = fma_rn(px, nx, mul_rn(py, ny));
     double pperpx = px - ppar * nx;
     double pperpy = py - ppar * ny;
     double pnew = gam * (ppar + vE);
@@ -505,8 +535,8 @@ __device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, R tau, 
         }
         R p2 = R(0);
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) p2 += pf[d] * pf[d];
-        R E = sqrt(p2 + M * M);
+        for (int d = 0; d < PDIM; ++d) p2 = fma_rn(pf[d], pf[d], p2);
+        R E = sqrt(fma_rn(M, M, p2));
         R Ew = kp.rel ? E : M;
         if (kp.integrator == 1) {
             R a_half = R(1) + expm1_neg((M / (Ew * tau)) * (R(0.5) * dt));
@@ -521,7 +551,7 @@ __device__ __forceinline__ void langevin_kick(const KParams<R>& kp, R T, R tau, 
         R one_m_a2 = -em1 * (R(2) + em1);
         R amp = (dt > R(0) && x > R(0)) ? sqrt(T * Ew * one_m_a2) : R(0);
 #pragma unroll
-        for (int d = 0; d < PDIM; ++d) p[d] += (double)(em1 * pf[d] + amp * xi[d]);
+        for (int d = 0; d < PDIM; ++d) p[d] += (double)fma_rn(amp, xi[d], mul_rn(em1, pf[d]));   // the kick fused
         return;
     }
     R etaD = ok ? R(1) / tau : R(0);
@@ -583,9 +613,9 @@ __device__ __forceinline__ R invcdf_lookup(const KParams<R>& kp, uint32_t w, R T
     const R* b0 = kp.icdf + (size_t)jT * nU + iu;
     const R* b1 = b0 + nU;
     R v00 = __ldg(b0), v10 = __ldg(b0 + 1), v01 = __ldg(b1), v11 = __ldg(b1 + 1);
-    R c0 = v00 * (R(1) - tu) + v10 * tu;
-    R c1 = v01 * (R(1) - tu) + v11 * tu;
-    return c0 * (R(1) - tT) + c1 * tT;
+    R c0 = fma_rn(v10, tu, mul_rn(v00, R(1) - tu));
+    R c1 = fma_rn(v11, tu, mul_rn(v01, R(1) - tu));
+    return fma_rn(c1, tT, mul_rn(c0, R(1) - tT));
 }
 
 template <typename R, int MED, int DIMS>
@@ -729,9 +759,9 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
 #pragma unroll
         for (int d = 0; d < 3; ++d) pf_out[d] = (float)pr_[d];
     }
-    R E2 = m * m;
+    R E2 = mul_rn(m, m);
 #pragma unroll
-    for (int d = 0; d < PDIM; ++d) E2 += pr_[d] * pr_[d];
+    for (int d = 0; d < PDIM; ++d) E2 = fma_rn(pr_[d], pr_[d], E2);
     R E = kp.rel ? sqrt(E2) : m;
     const R r_max = kp.med.r_max, r_axis_eps = kp.med.r_axis_eps;
     if (DIMS == 1) {
@@ -931,10 +961,10 @@ __device__ __forceinline__ double temperature_fp64(const KParams<R>& kp, const S
         for (int k = 0; k < 2; ++k) {
             const float4* q = k ? s1 : s0;
             double a00 = __ldg(q).x, a10 = __ldg(q + 1).x, a01 = __ldg(q + md.gnx).x, a11 = __ldg(q + md.gnx + 1).x;
-            double c0 = a00 * (1.0 - wx) + a10 * wx, c1 = a01 * (1.0 - wx) + a11 * wx;
-            c[k] = c0 * (1.0 - wy) + c1 * wy;
+            // the FP64 path's interpolation (bilerp_rn, grid_combine), rounding for rounding
+            c[k] = lerp_rn(lerp_rn(a00, a10, wx), lerp_rn(a01, a11, wx), wy);
         }
-        T = c[0] * (1.0 - sr.wtd) + c[1] * sr.wtd;
+        T = lerp_rn(c[0], c[1], sr.wtd);
     }
     if (md.T_scale != R(1)) T *= (double)md.T_scale;
     return T;
@@ -1074,9 +1104,8 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
         }
     } else {
         float Ts;
-        if (MED == MED_GRID && carry) {      // the next step's rows at the new position
-            // (no screen where the next step starts a new time row: the FP64 test decides)
-            Ts = carry->kt == sr.kt ? (float)lerp_rn(carry->T0, carry->T1, sr.wt) * (float)kp.med.T_scale : -1.0f;
+        if (MED == MED_GRID && carry) {      // from the lookup at the new position (GridRows)
+            Ts = carry->T1;
         } else {
             Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
         }
