@@ -10,10 +10,11 @@ from .hydro import HydroRT, HydroXY
 from .transport import (GevInvTofm, fmGeV, build_juttner_invcdf, build_tau_drag_spline, build_tau_R_spline,
                         build_taun_current_spline, effective_DsT, eval_tau_n_spline, tau_drag, tau_n_main3)
 from .utils import append_thermal_pz, check_momentum_dims, sample_pz_conditional_juttner
-from . import capi, hydro, sharding, transport, utils, workloads
+from .pipeline import EnsembleStream
+from . import capi, hydro, pipeline, sharding, transport, utils, workloads
 
 __all__ = ["AbstractBackend", "B200Backend", "B200_GCBackend", "FreezeOut", "simulate_ensemble_bulk",
            "GevInvTofm", "fmGeV", "build_juttner_invcdf", "build_tau_drag_spline", "build_tau_R_spline",
            "build_taun_current_spline", "effective_DsT", "eval_tau_n_spline", "tau_drag", "tau_n_main3",
            "append_thermal_pz", "check_momentum_dims", "sample_pz_conditional_juttner", "capi", "HydroRT",
-           "HydroXY"]
+           "HydroXY", "EnsembleStream"]
