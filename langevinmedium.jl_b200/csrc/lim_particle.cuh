@@ -120,7 +120,7 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];
         }
         float pf[3];
-        cart_step<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
+        cart_step<REC, R, MED, DIMS, PDIM, kCarry>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
         if constexpr (kCarry) {
             const bool more = s + 1 < s1;
             int kn = sr.kt;

@@ -415,10 +415,10 @@ __device__ __forceinline__ double sqrt_f32_newton(double s)
 // kernels_cpu.jl:89-145 (to_lab = false) and :188-241 (to_lab = true).  The frame
 // change is evaluated in FP64 in both precisions: with the momentum held in FP64,
 // p_par - v E does not lose the LRF momentum to cancellation at large gamma, and no
-// FP32 rounding of the momentum enters the state (FP32 increments of the frame change
-// cost up to 1e-5 of relative error over a few hundred steps at gamma ~ 1.4).
-// gamma = 1/sqrt(1 - v^2 + 1e-10) of the clamped local speed (kernels_cpu.jl:100-104),
-// computed once per step for both frame changes.
+// FP32 rounding of the momentum enters the state.  (The FP32 freeze-out kernel on the
+// grid changes frames in FP32 below gamma = 2 instead, as an increment of the FP64
+// state: step_rest_frame_incr.)  gamma = 1/sqrt(1 - v^2 + 1e-10) of the clamped local
+// speed (kernels_cpu.jl:100-104), computed once per step for both frame changes.
 template <typename R>
 __device__ __forceinline__ double boost_gamma(const Local<R>& L)
 {
@@ -647,10 +647,10 @@ __device__ __forceinline__ bool rta_decide_fp64(const KParams<R>& kp, const Step
 // tn: the RTA relaxation time (0 when DsT <= 0 or T <= 0), kernels_gpu.jl:675-679.
 // wc: the collision word (uc = u_value<R>(wc)); sr, x, xl: the step record and the
 // pre-step position (for the FP32 path's near-threshold FP64 decision).
-template <int REC, typename R, int MED, int DIMS, int PDIM>
-__device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int64_t s, const NoiseKey& nk,
+template <int REC, typename R, int MED, int DIMS, int PDIM, typename PT = double>
+__device__ __forceinline__ bool rta_collide(const KParams<R>& kp, int64_t i, int64_t s, const NoiseKey& nk,
                                             R T, R tn, uint32_t wc, const StepRec<R>& sr, const R (&x)[3],
-                                            const float (&xl)[3], double (&p)[3])
+                                            const float (&xl)[3], PT (&p)[3])
 {
     const R uc = u_value<R>(wc);
     R Pcol = (tn > R(0) && isfinite(tn)) ? jclamp(kp.dtR / tn, R(0), R(1)) : R(1);
@@ -664,7 +664,7 @@ __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int
         if (kp.rta_mode == 2) collide = (*w & bit) != 0u;
         else if (collide) *w |= bit;
     }
-    if (!collide) return;
+    if (!collide) return false;
     const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_RTA);
     R pstar = invcdf_lookup(kp, u.x, T);
     R g[3];
@@ -673,14 +673,15 @@ __device__ __forceinline__ void rta_collide(const KParams<R>& kp, int64_t i, int
     rec_slot<REC>(kp, s, i, 4, u_exact(u.x));
 #pragma unroll
     for (int d = 0; d < 3; ++d) rec_slot<REC>(kp, s, i, 5 + d, g[d]);
-    if (DIMS == 1) { p[0] = (double)((g[0] < R(0) ? R(-1) : R(1)) * pstar); return; }
+    if (DIMS == 1) { p[0] = (PT)((g[0] < R(0) ? R(-1) : R(1)) * pstar); return true; }
     R nrm2 = R(0);
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) nrm2 += g[d] * g[d];
     const R tiny = (R)(sizeof(R) == 8 ? 1e-300 : 1e-30);   // the reference's 1e-300 guard, FP32-representable
     R inv = pstar / sqrt(nrm2 > tiny ? nrm2 : tiny);
 #pragma unroll
-    for (int d = 0; d < PDIM; ++d) p[d] = (double)(g[d] * inv);
+    for (int d = 0; d < PDIM; ++d) p[d] = (PT)(g[d] * inv);
+    return true;
 }
 
 // kernels_cpu.jl:671-735 (momentum_langevin = false or DsT == 0).
@@ -837,9 +838,122 @@ __device__ __forceinline__ void stream_positions(const KParams<R>& kp, const Ste
     }
 }
 
+// FP32 step on the 2+1D grid with the frame changes as FP32 increments (flow speed
+// below kVIncr, gamma <= 2; faster flows take the FP64 frame change of cart_step).  The
+// lab momentum p stays FP64.  The rest-frame momentum p* = L(p) is formed in FP32 from
+// p rounded to FP32 (kernels_cpu.jl:89-145); the Bjorken redshift of its p_z, the kick
+// and the RTA resample change it by dl (FP32, as in cart_step); the lab momentum then
+// moves by
+//     L^-1(p* + dl) - L^-1(p*) = dl + n [(gamma - 1) (dl . n) + gamma v (E1 - E0)],
+// E1 - E0 = dl . (2 p* + dl) / (E1 + E0), the exact difference of the two lab-frame
+// changes (kernels_cpu.jl:188-241) without cancellation, added to p in FP64.  The FP32
+// rounding of p* enters only the increment, so the state keeps the FP64 frame change's
+// accuracy at a fraction of its FP64 work.
+constexpr float kVIncr = 0.8660254f;   // gamma = 2
+
+template <int REC, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void step_rest_frame_incr(const KParams<float>& kp, const StepRec<float>& sr, int64_t i,
+                                                     int64_t s, const NoiseKey& nk, const float (&x)[3],
+                                                     const float (&xl)[3], double (&p)[3], const Local<float>& L)
+{
+    const float m = kp.m;
+    float pl[3] = { 0.0f, 0.0f, 0.0f };
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) pl[d] = (float)p[d];
+    const float v = L.v, vv = mul_rn(v, v);
+    const float g = rsqrtf(1.0f - vv);
+    const float gm1 = __fdividef(mul_rn(vv, mul_rn(g, g)), 1.0f + g);     // gamma - 1 = gamma^2 v^2 / (1 + gamma)
+    const float gv = mul_rn(g, v);
+    const float nx = L.nx, ny = L.ny;
+    float q = mul_rn(m, m);
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) q = fma_rn(pl[d], pl[d], q);
+    const float El = sqrtf(q);
+    const float dpar = fma_rn(gm1, fma_rn(pl[0], nx, mul_rn(pl[1], ny)), -mul_rn(gv, El));
+    float ps[3] = { fma_rn(dpar, nx, pl[0]), fma_rn(dpar, ny, pl[1]), pl[2] };
+    float E0 = mul_rn(m, m);
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) E0 = fma_rn(ps[d], ps[d], E0);
+    E0 = sqrtf(E0);
+    // the change dl of p*, kept apart from p* so that its FP32 rounding is that of the
+    // change: the redshift of p*_z (kernels_cpu.jl:427-435), then the kick on the
+    // redshifted p* (pr), or the RTA resample in place of both
+    float dl[3] = { 0.0f, 0.0f, 0.0f };
+    float pr[3] = { ps[0], ps[1], ps[2] };
+    float Er = E0;
+    if (PDIM == 3 && kp.redshift) {
+        dl[2] = mul_rn((float)(sr.zf - 1.0), ps[2]);
+        pr[2] = ps[2] + dl[2];
+        float qr = mul_rn(m, m);
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) qr = fma_rn(pr[d], pr[d], qr);
+        Er = sqrtf(qr);
+    }
+    const float T = jmax0(L.T);
+    const uint4 u = philox_words(nk.rk, nk.pid, (uint32_t)s, TAG_MOM);
+    const bool kick = kp.collision != COLL_RTA;
+    const bool rta = kp.collision == COLL_RTA || kp.collision == COLL_LANGEVIN_RTA;
+    const SplIdx<float> sd = spline_index(T, kp.drag_Tmin, kp.drag_invdT, kp.n_drag);
+    uint32_t wc = u.x;
+    if (kick) {
+        float xi[3];
+        box_muller(u.x, u.y, xi[0], xi[1]);
+        if (PDIM == 3) { xi[2] = norm_inv(u.z, 0.0f); wc = u.w; }
+        else { xi[2] = 0.0f; wc = u.z; }
+#pragma unroll
+        for (int d = 0; d < PDIM; ++d) rec_slot<REC>(kp, s, i, d, xi[d]);
+        const float tau = kp.DsT <= 0.0f ? 0.0f : spline_at(kp.drag, sd);
+        const float M = m, dt = kp.dtR;
+        if (tau > 0.0f && isfinite(tau)) {               // as langevin_kick's FP32 form, on p*
+            float Ew = Er;
+            if (kp.integrator == 1) {
+                const float a_half = 1.0f + expm1_neg((M / (Ew * tau)) * (0.5f * dt));
+                float p2m = 0.0f;
+#pragma unroll
+                for (int d = 0; d < PDIM; ++d) { const float qd = a_half * pr[d]; p2m += qd * qd; }
+                Ew = sqrtf(p2m + M * M);
+            }
+            const float xx = (M / (Ew * tau)) * dt;
+            const float em1 = expm1_neg(xx);
+            const float one_m_a2 = -em1 * (2.0f + em1);
+            const float amp = (dt > 0.0f && xx > 0.0f) ? sqrtf(T * Ew * one_m_a2) : 0.0f;
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) dl[d] += fma_rn(amp, xi[d], mul_rn(em1, pr[d]));
+        }
+    }
+    if (rta) {
+        rec_slot<REC>(kp, s, i, 3, u_exact(wc));
+        float tn = 0.0f;
+        if (kp.DsT > 0.0f && T > 0.0f)
+            tn = spline_at(kp.rta, kp.spl_shared ? sd : spline_index(T, kp.rta_Tmin, kp.rta_invdT, kp.n_rta));
+        float pc[3] = { 0.0f, 0.0f, 0.0f };
+        if (rta_collide<REC, float, MED, DIMS, PDIM, float>(kp, i, s, nk, T, tn, wc, sr, x, xl, pc)) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) dl[d] = pc[d] - ps[d];
+        }
+    }
+    float sm[3];
+    float E1 = mul_rn(m, m);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float pn = ps[d] + dl[d];
+        sm[d] = ps[d] + pn;
+        if (d < PDIM) E1 = fma_rn(pn, pn, E1);
+    }
+    E1 = sqrtf(E1);
+    float dd = mul_rn(dl[0], sm[0]);
+#pragma unroll
+    for (int d = 1; d < PDIM; ++d) dd = fma_rn(dl[d], sm[d], dd);
+    const float dE = __fdividef(dd, E0 + E1);
+    const float c = fma_rn(gm1, fma_rn(dl[0], nx, mul_rn(dl[1], ny)), mul_rn(gv, dE));
+    p[0] += (double)fma_rn(c, nx, dl[0]);
+    p[1] += (double)fma_rn(c, ny, dl[1]);
+    if (PDIM == 3) p[2] += (double)dl[2];
+}
+
 // One Cartesian step (simulate_cpu.jl:215-290).
 // pf_out (optional): the lab momentum after the step, rounded to FP32.
-template <int REC, typename R, int MED, int DIMS, int PDIM>
+template <int REC, typename R, int MED, int DIMS, int PDIM, bool INCR = false>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3],
                                           GridRows<R>* carry = nullptr, float* pf_out = nullptr)
@@ -855,6 +969,13 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
         trow[0] = make_float4((float)p[0], (float)p[1], (float)p[2], mg.T);
         trow[2 * kp.n] = make_float4(mg.vy, mg.dT[0], mg.dT[1], mg.dvx[0]);
         trow[3 * kp.n] = make_float4(mg.dvx[1], mg.dvy[0], mg.dvy[1], 0.0f);
+    }
+    if constexpr (INCR && MED == MED_GRID && sizeof(R) == 4 && DIMS == 2) {
+        if (kp.rel && kp.collision != COLL_FLUID && L.v < kVIncr) {
+            step_rest_frame_incr<REC, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, L);
+            stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, pf_out);
+            return;
+        }
     }
     // on the grid gamma is computed once for both frame changes (measured 2 % faster
     // there; the (r, t) and Bjorken kernels keep their own form, measured faster for them)
