@@ -111,6 +111,12 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
         const R w0 = tab[s0].wt;
         grid_combine(rows, w0, rows.T0, rows.U0, rows.V0);
     }
+    // the lab momentum rounded to FP32, as streaming leaves it at the end of each step: the
+    // FP32 grid kernel's next step starts its frame change from it (the same values as
+    // rounding p again)
+    float pf[3] = { 0.0f, 0.0f, 0.0f };
+#pragma unroll
+    for (int d = 0; d < PDIM; ++d) pf[d] = (float)p[d];
     for (int64_t s = s0; s < s1; ++s) {
         if (FO && kp.stop_fo && frozen) break;
         const StepRec<R> sr = tab[s];
@@ -119,7 +125,6 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             *t = make_float4((float)x[0], (float)x[1], (float)p[0], (float)p[1]);
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];
         }
-        float pf[3];
         cart_step<REC, R, MED, DIMS, PDIM, kCarry>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
         if constexpr (kCarry) {
             const bool more = s + 1 < s1;

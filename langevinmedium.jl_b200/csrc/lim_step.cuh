@@ -854,12 +854,13 @@ constexpr float kVIncr = 0.8660254f;   // gamma = 2
 template <int REC, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void step_rest_frame_incr(const KParams<float>& kp, const StepRec<float>& sr, int64_t i,
                                                      int64_t s, const NoiseKey& nk, const float (&x)[3],
-                                                     const float (&xl)[3], double (&p)[3], const Local<float>& L)
+                                                     const float (&xl)[3], double (&p)[3], const Local<float>& L,
+                                                     const float* pin)
 {
     const float m = kp.m;
-    float pl[3] = { 0.0f, 0.0f, 0.0f };
+    float pl[3] = { 0.0f, 0.0f, 0.0f };           // p rounded to FP32 (pin: the caller's copy)
 #pragma unroll
-    for (int d = 0; d < PDIM; ++d) pl[d] = (float)p[d];
+    for (int d = 0; d < PDIM; ++d) pl[d] = pin ? pin[d] : (float)p[d];
     const float v = L.v, vv = mul_rn(v, v);
     const float g = rsqrtf(1.0f - vv);
     const float gm1 = __fdividef(mul_rn(vv, mul_rn(g, g)), 1.0f + g);     // gamma - 1 = gamma^2 v^2 / (1 + gamma)
@@ -952,7 +953,9 @@ __device__ __forceinline__ void step_rest_frame_incr(const KParams<float>& kp, c
 }
 
 // One Cartesian step (simulate_cpu.jl:215-290).
-// pf_out (optional): the lab momentum after the step, rounded to FP32.
+// pf_out (optional): the lab momentum after the step, rounded to FP32; with INCR (the
+// FP32 grid freeze-out kernel) it holds the lab momentum before the step, rounded the
+// same way, on entry.
 template <int REC, typename R, int MED, int DIMS, int PDIM, bool INCR = false>
 __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                           const NoiseKey& nk, R (&x)[3], float (&xl)[3], double (&p)[3],
@@ -972,7 +975,7 @@ __device__ __forceinline__ void cart_step(const KParams<R>& kp, const StepRec<R>
     }
     if constexpr (INCR && MED == MED_GRID && sizeof(R) == 4 && DIMS == 2) {
         if (kp.rel && kp.collision != COLL_FLUID && L.v < kVIncr) {
-            step_rest_frame_incr<REC, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, L);
+            step_rest_frame_incr<REC, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, L, pf_out);
             stream_positions<REC, R, MED, DIMS, PDIM>(kp, sr, i, s, nk, x, xl, p, pf_out);
             return;
         }
