@@ -125,6 +125,11 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             *t = make_float4((float)x[0], (float)x[1], (float)p[0], (float)p[1]);
             reinterpret_cast<float*>(t + kp.n)[0] = (float)p[2];
         }
+        // FP32 latch: the state the step starts from is the last-above record
+        R xp[3];
+        float xlp[3], pfp[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { xp[d] = x[d]; xlp[d] = xl[d]; pfp[d] = pf[d]; }
         cart_step<REC, R, MED, DIMS, PDIM, kCarry>(kp, sr, i, s, nk, x, xl, p, carry, FO && sizeof(R) == 4 ? pf : nullptr);
         if constexpr (kCarry) {
             const bool more = s + 1 < s1;
@@ -136,17 +141,22 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
             if (more) grid_combine(rows, wn, rows.T0, rows.U0, rows.V0);
             rows.T1 = scr;
         }
-        if (FO) freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last,
-                                                    carry);
+        if constexpr (FO && sizeof(R) == 4) {
+            freezeout_latch_pre<R, MED, DIMS, PDIM>(kp, sr, i, s, x, xl, p, xp, xlp, pfp, frozen, have_last, carry);
+        } else if (FO) {
+            freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last, carry);
+        }
         if (!state_finite<R, DIMS, PDIM>(kp, x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
             break;
         }
     }
     store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    if (FO) {
+    if (FO && sizeof(R) == 4) {
+        kp.l_T[i] = have_last ? -1.0 : 0.0;      // the record is the state itself (freezeout_latch_pre)
+    } else if (FO) {
         kp.l_tau[i] = ltau;
-        kp.l_T[i] = sizeof(R) == 4 ? (have_last ? -1.0 : 0.0) : lT;
+        kp.l_T[i] = lT;
 #pragma unroll
         for (int d = 0; d < DIMS; ++d) kp.l_pos[d][i] = lpos.at(d);
 #pragma unroll

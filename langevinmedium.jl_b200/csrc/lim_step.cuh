@@ -1266,6 +1266,57 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
     }
 }
 
+// The FP32 freeze-out latch without a last-above record.  A particle that is not frozen
+// at step s was above Tfo after every step before (else it would have latched there), so
+// its last-above state is the state before step s: the position pair (xp, xlp), the lab
+// momentum as streaming rounded it (pfp) and the time of step s - 1.  The caller keeps
+// them through the step (they are the registers the step starts from) instead of a
+// record copied every step.  have_last: the particle has run a step before this one.
+// Otherwise as freezeout_latch's FP32 path: the FP32 screen, the FP64 test within kScreen
+// of Tfo, the crossing interpolated in FP64, and the last-above temperature re-evaluated
+// in FP64 at the crossing from the same position and time, so the same bits.
+template <typename R, int MED, int DIMS, int PDIM>
+__device__ __forceinline__ void freezeout_latch_pre(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
+                                                    const R (&x)[3], const float (&xl)[3], const double (&p)[3],
+                                                    const R (&xp)[3], const float (&xlp)[3], const float (&pfp)[3],
+                                                    bool& frozen, bool& have_last, const GridRows<R>* carry)
+{
+    constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
+    if (frozen) return;
+    const double Tfo = (double)kp.Tfo;
+    float Ts;
+    if (MED == MED_GRID && carry) Ts = carry->T1;      // from the lookup at the new position (GridRows)
+    else Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
+    if (!(Ts >= (float)Tfo + kScreen)) {
+        double xd[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (double)xl[d];
+        const double T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
+        if (T < Tfo) {
+            double lp[3] = { 0.0, 0.0, 0.0 }, lm[3] = { 0.0, 0.0, 0.0 }, lt = 0.0, lTv = 0.0;
+            if (have_last) {
+#pragma unroll
+                for (int d = 0; d < DIMS; ++d) lp[d] = (double)xp[d] + (double)xlp[d];
+#pragma unroll
+                for (int d = 0; d < PDIM; ++d) lm[d] = (double)pfp[d];
+                lt = step_time(kp, s - 1);
+                const StepRec<R> pr = step_rec_at_time<R, MED>(kp, lt);
+                lTv = temperature_fp64<R, MED, DIMS>(kp, pr, lp);
+            }
+            const double frac = (kp.fo_interp && lTv > Tfo && lTv > T) ? (lTv - Tfo) / (lTv - T) : 1.0;
+#pragma unroll
+            for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lp[d] + frac * (xd[d] - lp[d]);
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lm[d] + frac * (p[d] - lm[d]);
+            kp.fo_tau[i] = lt + frac * (sr.t - lt);
+            kp.fo_flag[i] = 1.0;
+            frozen = true;
+            return;
+        }
+    }
+    have_last = true;
+}
+
 // ---------------------------------------------------------------------------
 // Milne (tau, r) step (simulate_cpu_general_coords.jl:83-126).  The Milne
 // interpolation neither clamps the query nor guards dx (kernels_cpu_GC.jl:37-57).
