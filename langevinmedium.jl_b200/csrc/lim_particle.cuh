@@ -78,20 +78,20 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     LatchPos<R> lpos;
     LatchMom<R> lmom;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { lpos.h[d] = R(0); lpos.l[d] = 0.0f; lmom.m[d] = 0; }
+    for (int d = 0; d < 3; ++d) { lpos.h[d] = R(0); lmom.m[d] = 0.0; }
     if (FO) {
-        // the latch record of the previous launch; l_T = 0 until a particle has one (in FP32
-        // runs the record holds -1 there and the temperature is re-evaluated at the crossing)
-        frozen = kp.fo_flag[i] != 0.0; ltau = kp.l_tau[i]; lT = kp.l_T[i];
+        // the latch state of the previous launch: l_T = 0 until a particle has a last-above
+        // state (FP32 runs hold -1 there; their last-above state is the state itself)
+        frozen = kp.fo_flag[i] != 0.0;
+        lT = kp.l_T[i];
         have_last = lT != 0.0;
+        if (sizeof(R) == 8) {
+            ltau = kp.l_tau[i];
 #pragma unroll
-        for (int d = 0; d < DIMS; ++d) {
-            const double v = kp.l_pos[d][i];   // FP32: split back into the pair it was stored from
-            lpos.h[d] = (R)v;
-            if (sizeof(R) == 4) lpos.l[d] = (float)(v - (double)lpos.h[d]);
+            for (int d = 0; d < DIMS; ++d) lpos.h[d] = (R)kp.l_pos[d][i];
+#pragma unroll
+            for (int d = 0; d < PDIM; ++d) lmom.m[d] = kp.l_mom[d][i];
         }
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) lmom.m[d] = kp.l_mom[d][i];
     }
     const NoiseKey nk{ rk, (uint32_t)(kp.pid_offset + i) };
     const StepRec<R>* __restrict__ tab = (const StepRec<R>*)kp.steps - kp.step_base;
@@ -143,8 +143,8 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
         }
         if constexpr (FO && sizeof(R) == 4) {
             freezeout_latch_pre<R, MED, DIMS, PDIM>(kp, sr, i, s, x, xl, p, xp, xlp, pfp, frozen, have_last, carry);
-        } else if (FO) {
-            freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, xl, p, pf, frozen, lpos, lmom, ltau, lT, have_last, carry);
+        } else if constexpr (FO) {
+            freezeout_latch<R, MED, DIMS, PDIM>(kp, sr, i, x, p, frozen, lpos, lmom, ltau, lT);
         }
         if (!state_finite<R, DIMS, PDIM>(kp, x, p)) {
             atomicMin(kp.first_bad, (unsigned long long)s);
@@ -152,9 +152,9 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
         }
     }
     store_state<R, DIMS, PDIM>(kp, i, x, xl, p);
-    if (FO && sizeof(R) == 4) {
+    if constexpr (FO && sizeof(R) == 4) {
         kp.l_T[i] = have_last ? -1.0 : 0.0;      // the record is the state itself (freezeout_latch_pre)
-    } else if (FO) {
+    } else if constexpr (FO) {
         kp.l_tau[i] = ltau;
         kp.l_T[i] = lT;
 #pragma unroll

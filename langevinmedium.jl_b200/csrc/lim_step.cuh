@@ -1154,115 +1154,60 @@ __device__ __forceinline__ float temperature_screen(const KParams<R>& kp, const 
     return (float)temperature_at<R, MED, DIMS>(kp, sr, x, r);
 }
 
-// The latch's last-above position: in FP64 runs the position itself; in FP32 runs the
-// FP32 pair (x, x_lo) it was recorded from, summed in FP64 only where the position is
-// used (the same sum the record would have taken, so the same bits), which spares the
-// conversions on every step the particle stays above.
+// The FP64 latch's last-above record: the position and the lab momentum of the last
+// step the particle ended above Tfo (FP64 runs; the FP32 kernels keep no record,
+// freezeout_latch_pre).
 template <typename R>
 struct LatchPos {
     R h[3];
-    float l[3];
-    __device__ __forceinline__ double at(int d) const
-    {
-        if constexpr (sizeof(R) == 8) return h[d];
-        else return (double)h[d] + (double)l[d];
-    }
+    __device__ __forceinline__ double at(int d) const { return (double)h[d]; }
 };
 
-// The latch's last-above momentum: FP64 in FP64 runs; in FP32 runs the step's lab
-// momentum rounded to FP32 (the latch interpolates it with the current FP64 momentum,
-// so its rounding reaches the latched momentum at 6e-8 relative).
 template <typename R>
 struct LatchMom {
-    typename std::conditional<sizeof(R) == 8, double, float>::type m[3];
-    __device__ __forceinline__ double at(int d) const { return (double)m[d]; }
+    double m[3];
+    __device__ __forceinline__ double at(int d) const { return m[d]; }
 };
 
-// Freeze-out latch after streaming (kernels_gpu.jl:588-635), evaluated in FP64.
-// FP64 path: the temperature at the particle in FP64 every step; the last-above
-// temperature lT is kept.  FP32 path: the FP64 temperature is evaluated only when an
-// FP32 screen puts T within kScreen of Tfo; the last-above temperature is not kept but
-// re-evaluated in FP64 from the recorded position and time at the crossing (the same
-// evaluation as at that step, so the same bits); have_last tells whether there is a
-// last-above record at all (a particle already below Tfo at its first step latches with
-// frac = 1, as with lT = 0 in the reference).  pf: the step's lab momentum in FP32.
+// Freeze-out latch after streaming (kernels_gpu.jl:588-635), FP64 runs: the temperature
+// at the particle in FP64 every step; the last-above state and temperature lT are kept
+// (a particle already below Tfo at its first step latches with frac = 1, as with lT = 0
+// in the reference).
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const StepRec<R>& sr, int64_t i,
-                                                const R (&x)[3], const float (&xl)[3], const double (&p)[3],
-                                                const float (&pf)[3], bool& frozen, LatchPos<R>& lpos,
-                                                LatchMom<R>& lmom, double& ltau, double& lT, bool& have_last,
-                                                GridRows<R>* carry = nullptr)
+                                                const R (&x)[3], const double (&p)[3], bool& frozen,
+                                                LatchPos<R>& lpos, LatchMom<R>& lmom, double& ltau, double& lT)
 {
-    constexpr float kScreen = 1e-4f;     // GeV; FP32 and FP64 temperatures differ by < 1e-6
+    static_assert(sizeof(R) == 8, "the FP32 kernels latch with freezeout_latch_pre");
     if (frozen) return;
     const double Tfo = (double)kp.Tfo;
     double T;
-    if constexpr (sizeof(R) == 8) {
-        double xd[3];
+    double xd[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) xd[d] = (double)x[d];
-        R r;
-        if (DIMS == 1) r = fabs(x[0]);
-        else { R r2 = R(0);
+    for (int d = 0; d < 3; ++d) xd[d] = (double)x[d];
+    R r;
+    if (DIMS == 1) r = fabs(x[0]);
+    else { R r2 = R(0);
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
-            r = sqrt(r2); }
-        T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
-        if (T < Tfo) {
-            const double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
+        for (int d = 0; d < DIMS; ++d) r2 += x[d] * x[d];
+        r = sqrt(r2); }
+    T = (double)temperature_at<R, MED, DIMS>(kp, sr, x, r);
+    if (T < Tfo) {
+        const double frac = (kp.fo_interp && lT > Tfo && lT > T) ? (lT - Tfo) / (lT - T) : 1.0;
 #pragma unroll
-            for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
+        for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
 #pragma unroll
-            for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom.at(d) + frac * (p[d] - lmom.at(d));
-            kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
-            kp.fo_flag[i] = 1.0;
-            frozen = true;
-        } else {
-#pragma unroll
-            for (int d = 0; d < DIMS; ++d) lpos.h[d] = xd[d];
-#pragma unroll
-            for (int d = 0; d < PDIM; ++d) lmom.m[d] = p[d];
-            ltau = sr.t;
-            lT = T;
-            have_last = true;
-        }
+        for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom.at(d) + frac * (p[d] - lmom.at(d));
+        kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
+        kp.fo_flag[i] = 1.0;
+        frozen = true;
     } else {
-        float Ts;
-        if (MED == MED_GRID && carry) {      // from the lookup at the new position (GridRows)
-            Ts = carry->T1;
-        } else {
-            Ts = temperature_screen<R, MED, DIMS>(kp, sr, x);
-        }
-        if (!(Ts >= (float)Tfo + kScreen)) {
-            double xd[3];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) xd[d] = (double)x[d] + (double)xl[d];
-            T = temperature_fp64<R, MED, DIMS>(kp, sr, xd);
-            if (T < Tfo) {
-                double lTv = 0.0;
-                if (have_last) {
-                    const StepRec<R> pr = step_rec_at_time<R, MED>(kp, ltau);
-                    const double lp[3] = { lpos.at(0), lpos.at(1), lpos.at(2) };
-                    lTv = temperature_fp64<R, MED, DIMS>(kp, pr, lp);
-                }
-                const double frac = (kp.fo_interp && lTv > Tfo && lTv > T) ? (lTv - Tfo) / (lTv - T) : 1.0;
+        for (int d = 0; d < DIMS; ++d) lpos.h[d] = xd[d];
 #pragma unroll
-                for (int d = 0; d < DIMS; ++d) kp.fo_pos[d][i] = lpos.at(d) + frac * (xd[d] - lpos.at(d));
-#pragma unroll
-                for (int d = 0; d < PDIM; ++d) kp.fo_mom[d][i] = lmom.at(d) + frac * (p[d] - lmom.at(d));
-                kp.fo_tau[i] = ltau + frac * (sr.t - ltau);
-                kp.fo_flag[i] = 1.0;
-                frozen = true;
-                return;
-            }
-        }
-        // above Tfo: remember this step (position pair, FP32 momentum, time)
-#pragma unroll
-        for (int d = 0; d < DIMS; ++d) { lpos.h[d] = x[d]; lpos.l[d] = xl[d]; }
-#pragma unroll
-        for (int d = 0; d < PDIM; ++d) lmom.m[d] = pf[d];
+        for (int d = 0; d < PDIM; ++d) lmom.m[d] = p[d];
         ltau = sr.t;
-        have_last = true;
+        lT = T;
     }
 }
 
@@ -1271,10 +1216,12 @@ __device__ __forceinline__ void freezeout_latch(const KParams<R>& kp, const Step
 // its last-above state is the state before step s: the position pair (xp, xlp), the lab
 // momentum as streaming rounded it (pfp) and the time of step s - 1.  The caller keeps
 // them through the step (they are the registers the step starts from) instead of a
-// record copied every step.  have_last: the particle has run a step before this one.
-// Otherwise as freezeout_latch's FP32 path: the FP32 screen, the FP64 test within kScreen
-// of Tfo, the crossing interpolated in FP64, and the last-above temperature re-evaluated
-// in FP64 at the crossing from the same position and time, so the same bits.
+// record copied every step.  have_last: the particle has run a step before this one (a
+// particle already below Tfo at its first step latches with frac = 1).  The temperature
+// is screened in FP32 (kScreen: FP32 and FP64 temperatures differ by < 1e-6) and tested
+// in FP64 only near Tfo; at a crossing the last-above temperature is evaluated in FP64
+// from the pre-step position and the time of step s - 1, the crossing interpolated in
+// FP64 (frac = (T_last - Tfo)/(T_last - T)).
 template <typename R, int MED, int DIMS, int PDIM>
 __device__ __forceinline__ void freezeout_latch_pre(const KParams<R>& kp, const StepRec<R>& sr, int64_t i, int64_t s,
                                                     const R (&x)[3], const float (&xl)[3], const double (&p)[3],
