@@ -117,7 +117,9 @@ __device__ __forceinline__ void cart_particle(const KParams<R>& kp, const uint2*
     float pf[3] = { 0.0f, 0.0f, 0.0f };
 #pragma unroll
     for (int d = 0; d < PDIM; ++d) pf[d] = (float)p[d];
-    for (int64_t s = s0; s < s1; ++s) {
+    // steps lie in [0, 2^32) (lim_run checks): a 32-bit loop counter
+    const uint32_t se = (uint32_t)s1;
+    for (uint32_t s = (uint32_t)s0; s < se; ++s) {
         if (FO && kp.stop_fo && frozen) break;
         const StepRec<R> sr = tab[s];
         if (REC == 2 && MED != MED_GRID) {   // the adjoint's tape: the pre-step state (the normals follow)

@@ -193,15 +193,18 @@ template <typename R>
 __device__ __forceinline__ void grid_cell(const MediumDev<R>& md, R xq, R yq, int& ix, int& iy, R& wx, R& wy,
                                           float xlo = 0.0f, float ylo = 0.0f)
 {
-    R x = xq > (R)md.gxl_d ? (R)md.gxl_d : (xq < (R)md.gx0_d ? (R)md.gx0_d : xq);
-    R y = yq > (R)md.gyl_d ? (R)md.gyl_d : (yq < (R)md.gy0_d ? (R)md.gy0_d : yq);
     if constexpr (sizeof(R) == 4) {
+        // the query clamped to the grid through its cell: off the grid the cell index is
+        // clamped to the edge cell and the weight to 0 or 1, the edge node's value exactly
+        // (inside the grid nothing is clamped)
         float fwx, fwy;
-        cell_fp32(x, x == xq ? xlo : 0.0f, md.gicx, md.gxc, md.gxcl, md.ginvdx, md.ginvdx_lo, md.gnx, ix, fwx);
-        cell_fp32(y, y == yq ? ylo : 0.0f, md.gicy, md.gyc, md.gycl, md.ginvdy, md.ginvdy_lo, md.gny, iy, fwy);
-        wx = fwx;
-        wy = fwy;
+        cell_fp32(xq, xlo, md.gicx, md.gxc, md.gxcl, md.ginvdx, md.ginvdx_lo, md.gnx, ix, fwx);
+        cell_fp32(yq, ylo, md.gicy, md.gyc, md.gycl, md.ginvdy, md.ginvdy_lo, md.gny, iy, fwy);
+        wx = fminf(fmaxf(fwx, 0.0f), 1.0f);
+        wy = fminf(fmaxf(fwy, 0.0f), 1.0f);
     } else {
+        R x = xq > (R)md.gxl_d ? (R)md.gxl_d : (xq < (R)md.gx0_d ? (R)md.gx0_d : xq);
+        R y = yq > (R)md.gyl_d ? (R)md.gyl_d : (yq < (R)md.gy0_d ? (R)md.gy0_d : yq);
         R fx = (x - (R)md.gx0_d) / (R)md.gdx_d, fy = (y - (R)md.gy0_d) / (R)md.gdy_d;
         R flx = floor(fx), fly = floor(fy);
         ix = flx < R(0) ? 0 : (flx > R(md.gnx - 2) ? md.gnx - 2 : (int)flx);
