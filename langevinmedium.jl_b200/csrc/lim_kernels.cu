@@ -44,15 +44,14 @@ template <bool REC, int DIMS, int PDIM>
 __global__ void __launch_bounds__(128, 7)
 k_cart_grid_fo32(const KParams<float> kp, int64_t s0, int64_t s1)
 {
-    if (kp.live) {
-        const unsigned cnt = *kp.live_n;
-        for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x)
-            cart_particle<REC, true, float, MED_GRID, DIMS, PDIM>(kp, kp.rk, kp.live[k], s0, s1);
-        return;
+    // one inlined copy of the particle loop for both forms (the live list, or every
+    // particle with the grid covering them): half the code of two copies
+    const int64_t cnt = kp.live ? (int64_t)*kp.live_n : kp.n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += stride) {
+        const int64_t i = kp.live ? (int64_t)kp.live[k] : k;
+        cart_particle<REC, true, float, MED_GRID, DIMS, PDIM>(kp, kp.rk, i, s0, s1);
     }
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kp.n) return;
-    cart_particle<REC, true, float, MED_GRID, DIMS, PDIM>(kp, kp.rk, i, s0, s1);
 }
 
 // Ordered-within-block compaction of the particles whose freeze-out flag is clear:
