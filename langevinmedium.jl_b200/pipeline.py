@@ -5,7 +5,7 @@ a large sample) one ``simulate_ensemble_bulk`` call at a time pays, per ensemble
 upload of its initial state and the download of its results on top of the run: for
 the 2+1D grid workload (1e7 particles, FP64 host arrays in the reference's
 column-major layout) 400 MB in and 560 MB out, about 16 ms over PCIe against a
-114 ms run.  ``EnsembleStream`` keeps two slots of engine contexts, each on its own
+92 ms run.  ``EnsembleStream`` keeps two slots of engine contexts, each on its own
 CUDA stream: while the ensemble of pass k runs in one slot, the other slot downloads
 the outputs of pass k - 1 and uploads (and boosts to the lab frame) the initial state
 of pass k + 1, so the copies go through the copy engines under the run.  Runs never
